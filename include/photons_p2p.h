@@ -1,0 +1,152 @@
+/*
+ * photons_p2p.h - C ABI of libphotons_p2p.so, the B200 (sm_100a) TreePM
+ * short-range particle-particle (P2P) force pass.
+ *
+ * Plain pointers and sizes, no CUDA or C++ types in the signatures. Every
+ * function returns a status (P2P_OK = 0) and records a message readable with
+ * p2p_last_error(). Nothing here exits the process; the legacy PhotoNs entry
+ * points built on top of it (photons_gpu_entry.h) keep the reference's
+ * print-and-exit behaviour.
+ *
+ * The pass protocol mirrors the reference's task_compute_p2p_gpu call
+ * sequence (src/gpu_entry.cu:32-209, src/fmm.c:500-515 and :1275,
+ * src/gravity.c:440-449):
+ *   p2p_pass_begin        first call of a pass: particles + leaves uploaded,
+ *                         device accumulator zeroed    (src/gpu_entry.cu:82-122)
+ *   p2p_pass_submit       one list chunk: uploaded, CSR built on the device,
+ *                         kernel launched, returns before the GPU finishes
+ *                                                       (src/gpu_entry.cu:124-191)
+ *   p2p_pass_end          completion barrier, GPU seconds of the pass
+ *                                                       (get_last_kntime, src/gpu_func.impl.h:715-730)
+ *   p2p_pass_accumulate   acc[d][i] += result           (devMemcpyDH_updateAcc,
+ *                                                        src/gpu_func.impl.h:644-681)
+ * Leaf ids in task lists are 0-based (first_leaf already subtracted, as
+ * devMemcpyHD_task does, src/gpu_func.impl.h:704-713). Positions and
+ * accelerations are SoA: x[0..npart), y[0..npart), z[0..npart) - the
+ * d_part_pos / d_part_buf layout of the reference.
+ */
+#ifndef PHOTONS_P2P_H
+#define PHOTONS_P2P_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define P2P_OK 0
+#define P2P_ERR_ARG 1      /* invalid argument (null pointer, negative size, bad enum) */
+#define P2P_ERR_CUDA 2     /* a CUDA runtime call failed; see p2p_last_error() */
+#define P2P_ERR_STATE 3    /* call out of protocol order */
+#define P2P_ERR_NOMEM 4    /* device allocation failed */
+#define P2P_ERR_RANGE 5    /* a leaf id / particle range in the input was out of range;
+                              the offending entries were skipped, never dereferenced */
+#define P2P_ERR_CAPACITY 6 /* a fixed-capacity buffer is too small for the input */
+
+/* Softening (runtime choice; the reference fixes it per kernel). */
+#define P2P_SOFT_CLAMP 0   /* r < eps => r := eps (P2P_core_lite, src/gpu_kernel.impl.h:174-188) */
+#define P2P_SOFT_PLUMMER 1 /* r := sqrt(r^2 + eps^2) (P2P_core_1, src/gpu_kernel.impl.h:275-279) */
+
+/* Arithmetic forms of the pass. */
+#define P2P_FORM_PLAIN_FP64 0 /* FP64 throughout, CUDA erfc/exp: the drop-in form */
+#define P2P_FORM_SPLIT 1      /* FP32 leaf-local pair math, FP64 leaf offsets and
+                                 FP64 accumulation, fitted erfc polynomial: the chosen form */
+#define P2P_FORM_NAIVE_FP32 2 /* FP32 global coordinates, FP32 accumulation (precision study) */
+#define P2P_FORM_KAHAN_FP32 3 /* FP32 leaf-local math, Kahan-compensated FP32 accumulation */
+
+typedef struct {
+    int form;            /* P2P_FORM_* */
+    int soft_mode;       /* P2P_SOFT_* */
+    double soften;       /* SoftenScale (box units) */
+    double split_radius; /* splitRadius r_s (box units); x = r / (2 r_s) */
+    double x_cut;        /* pairs with x > x_cut contribute nothing (GPUCUTOFF uses
+                            2.8125, src/gpu_kernel.impl.h:192-196); <= 0: no cutoff */
+    double mass;         /* MASSPART: equal particle mass, used when no masses are given */
+    int warps_per_block; /* launch shape of the pair kernel; 0 = default */
+    int stage_sources;   /* sources staged per warp in shared memory; 0 = default */
+    int blocks_per_sm;   /* persistent grid = blocks_per_sm * SMs; 0 = default */
+    int reserved;
+} p2p_params;
+
+typedef struct p2p_session p2p_session;
+
+/* Fills params with the reference's defaults for the plain drop-in form:
+ * clamp softening, x_cut 2.8125, given soften / split radius / mass. */
+void p2p_params_default(p2p_params *params);
+
+const char *p2p_status_string(int status);
+/* Message of the last failing call on this thread ("" when none). */
+const char *p2p_last_error(void);
+/* Library version as major*10000 + minor*100 + patch. */
+int p2p_version(void);
+
+/* Number of CUDA devices visible to the process (0 when none). */
+int p2p_device_count(int *count);
+
+/* Sessions own the device buffers (grow-only) and one CUDA stream. */
+int p2p_session_create(int device, p2p_session **out);
+int p2p_session_destroy(p2p_session *s);
+int p2p_session_set_params(p2p_session *s, const p2p_params *params);
+int p2p_session_get_params(const p2p_session *s, p2p_params *params);
+/* The cudaStream_t (as void*) every launch of this session goes to. */
+void *p2p_session_stream(p2p_session *s);
+/* Degree of the fitted polynomial used by the FP32 forms (0 for FP64). */
+int p2p_session_poly_degree(const p2p_session *s);
+/* Max over the fitted range of x * |P(x^2) - H(x^2)| (H defined by
+ * g(x) = 1 - x^3 H(x^2)): the per-pair force error bound of the polynomial
+ * in units of the force at x = 1. */
+double p2p_session_poly_error(const p2p_session *s);
+
+/* First call of a pass. pos: 3*npart doubles (SoA, host). masses: npart
+ * doubles or NULL (equal mass params.mass). leaf_ipart/leaf_npart: nleaf
+ * ints, each leaf a range of particle slots [ipart, ipart+npart). */
+int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *masses,
+                   int nleaf, const int *leaf_ipart, const int *leaf_npart);
+/* Same with device pointers (already resident in HBM; not copied). */
+int p2p_pass_begin_device(p2p_session *s, int npart, const double *d_pos, const double *d_masses,
+                          int nleaf, const int *d_leaf_ipart, const int *d_leaf_npart);
+/* One chunk of the interaction list: ntask (sink, source) leaf-id pairs. */
+int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, const int *task_s);
+int p2p_pass_submit_device(p2p_session *s, int64_t ntask, const int *d_task_t, const int *d_task_s);
+/* Completion barrier; *gpu_seconds (nullable) = device time from begin to
+ * the last submitted chunk. Reports P2P_ERR_RANGE if any input was out of range. */
+int p2p_pass_end(p2p_session *s, double *gpu_seconds);
+/* acc[d*npart + i] += result (host SoA doubles). Call after p2p_pass_end. */
+int p2p_pass_accumulate(p2p_session *s, double *acc);
+/* out[d*npart + i] = result (host SoA doubles, copied). Call after p2p_pass_end. */
+int p2p_pass_result(p2p_session *s, double *out);
+/* Device pointer to the result (SoA doubles, 3*npart), valid until the next begin. */
+int p2p_pass_result_device(p2p_session *s, const double **d_acc);
+/* Pair-interaction count sum(n_sink * n_source) of the chunks submitted in
+ * the current pass, counted on the device (src/gpu_entry.cu:53-58). */
+int p2p_pass_pair_count(p2p_session *s, int64_t *pairs);
+
+/* Whole pass on device-resident inputs in one call, enqueued on the session
+ * stream without waiting: zero, prepare, CSR build, pair kernel. The launch
+ * sequence is captured once as a CUDA graph and replayed while the inputs
+ * (pointers and sizes) stay the same. Finish with p2p_pass_end. */
+int p2p_pass_run_device(p2p_session *s, int npart, const double *d_pos, const double *d_masses,
+                        int nleaf, const int *d_leaf_ipart, const int *d_leaf_npart,
+                        int64_t ntask, const int *d_task_t, const int *d_task_s);
+
+/* Waits for all work queued on the session stream. */
+int p2p_session_synchronize(p2p_session *s);
+
+/* Number of kernels this library has launched in the process (graph replays
+ * count each kernel node), for launch accounting. */
+int64_t p2p_kernel_launch_count(void);
+
+/* Duration in ms of the last pair-kernel launch of the session, measured with
+ * CUDA events on the session stream (0 if none). Call after p2p_pass_end. */
+int p2p_session_last_kernel_ms(p2p_session *s, float *ms);
+
+/* Measured FP32 FFMA throughput of this GPU (TFLOP/s, FMA = 2 flops) from a
+ * dependent-chain microbenchmark run on the session stream. */
+int p2p_measure_fp32_peak(p2p_session *s, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHOTONS_P2P_H */

@@ -1,0 +1,66 @@
+"""Build recipe for the native libraries of the package.
+
+    libphotons_p2p.so    CUDA P2P pass for sm_100a + its C ABI (csrc/*.cu)
+    libphotons_lists.so  host tree build / interaction-list walk (host/*.cpp)
+
+Both land in photons_p2p/ next to the Python bindings, so a snapshot of the
+repository carries them. Run `python photons-on-mt3000_b200/build.py`
+(add --force to rebuild). nvcc cross-compiles sm_100a without a GPU.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+OUT = os.path.join(HERE, "photons_p2p")
+INCLUDE = os.path.join(REPO, "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+CUDA_SOURCES = ["p2p_core.cu"]
+CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_internal.h"]
+HOST_SOURCES = ["p2p_lists.cpp"]
+
+GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def build_lists(force=False):
+    target = os.path.join(OUT, "libphotons_lists.so")
+    srcs = [os.path.join(HERE, "host", s) for s in HOST_SOURCES]
+    if force or _stale(target, srcs + [__file__]):
+        _run(["g++", "-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-fopenmp", "-shared",
+              "-o", target] + srcs)
+    return target
+
+
+def build_cuda(force=False, extra=()):
+    target = os.path.join(OUT, "libphotons_p2p.so")
+    srcs = [os.path.join(HERE, "csrc", s) for s in CUDA_SOURCES]
+    deps = srcs + [os.path.join(HERE, "csrc", h) for h in CUDA_HEADERS] + [
+        os.path.join(INCLUDE, "photons_p2p.h"), __file__]
+    if force or _stale(target, deps):
+        _run([NVCC] + GENCODE + ["-lineinfo", "-O3", "-std=c++17", "--shared",
+                                 "-Xcompiler", "-fPIC,-fvisibility=hidden",
+                                 "-I", INCLUDE, "-o", target] + list(extra) + srcs)
+    return target
+
+
+def build(force=False):
+    os.makedirs(OUT, exist_ok=True)
+    return [build_lists(force), build_cuda(force)]
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

@@ -1,0 +1,239 @@
+// PhotoNs gpu_entry boundary served by the B200 library (the drop-in for
+// src/gpu_entry.cu + src/gpu_func.impl.h). Compiled inside a PhotoNs source
+// tree, against its photoNs.h, with its -D flags:
+//   CPU_DP / INTXYZ   layout of Body (inc/typedef.h:24-46), as in PhotoNs
+//   GPU_DP            selects the plain FP64 form (default: the FP32/FP64
+//                     split form); PHOTONS_P2P_FORM=plain|split overrides
+//   GPUCUTOFF         pair cutoff x > 2.8125 (src/gpu_kernel.impl.h:192-196)
+// The functions read the same globals the reference's versions read and keep
+// its call protocol, ownership and print-and-exit error behaviour; the
+// declarations are listed in include/photons_gpu_entry.h.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+extern "C" {
+#include "photoNs.h"
+}
+#include "photons_p2p.h"
+
+namespace {
+
+p2p_session *g_sess = nullptr;
+int g_call_cnt = 0;
+long long g_tot_tasks = 0;
+bool g_pass_open = false;
+double *g_out = nullptr;  // h_part_buf of the reference
+int g_out_n = 0;
+
+[[noreturn]] void die(const char *where, int status) {
+    // checkDevErrors, src/gpu_func.impl.h:70-86
+    fprintf(stderr, "Device runtime error in %s: %s (%s)\n", where, p2p_status_string(status),
+            p2p_last_error());
+    exit(EXIT_FAILURE);
+}
+
+void check(const char *where, int status) {
+    if (status != P2P_OK) die(where, status);
+}
+
+int choose_form() {
+    const char *env = getenv("PHOTONS_P2P_FORM");
+    if (env && !strcmp(env, "plain")) return P2P_FORM_PLAIN_FP64;
+    if (env && !strcmp(env, "split")) return P2P_FORM_SPLIT;
+#ifdef GPU_DP
+    return P2P_FORM_PLAIN_FP64;
+#else
+    return P2P_FORM_SPLIT;
+#endif
+}
+
+// initGPU (src/gpu_func.impl.h:428-454, non-INTRA_LB): ranks share devices.
+void init_device() {
+    if (g_sess) return;
+    int ndev = 0;
+    check("p2p_device_count", p2p_device_count(&ndev));
+    if (ndev <= 0) {
+        printf("No available device\n");
+        exit(0);
+    }
+    int dev;
+    if (PROC_SIZE / ndev == 0)
+        dev = PROC_RANK;
+    else
+        dev = (PROC_RANK % PROC_SIZE) / (PROC_SIZE / ndev);
+    if (dev >= ndev) dev = dev % ndev;
+    check("p2p_session_create", p2p_session_create(dev, &g_sess));
+}
+
+void set_pass_params() {
+    p2p_params p;
+    p2p_params_default(&p);
+    p.form = choose_form();
+    p.soft_mode = P2P_SOFT_CLAMP;  // P2P_kernel3 calls P2P_core_lite
+    p.soften = SoftenScale;
+    p.split_radius = splitRadius;
+#ifdef GPUCUTOFF
+    p.x_cut = 2.8125;
+#else
+    p.x_cut = 0.0;
+#endif
+    p.mass = MASSPART;
+    check("p2p_session_set_params", p2p_session_set_params(g_sess, &p));
+}
+
+// SoA pack of the particle positions (src/gpu_entry.cu:85-105) and the leaf
+// table (:108-111), then the first-call upload (devMemcpyHD_part).
+void begin_pass() {
+    init_device();
+    set_pass_params();
+    const int n = NPART;
+    const int nleaf = last_leaf - first_leaf;
+    std::vector<double> pos(3 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) {
+#ifndef INTXYZ
+            pos[(size_t)d * n + i] = part[i].pos[d];
+#else
+            pos[(size_t)d * n + i] = INT2POS * (part[i].posi[d] - domain_center_i[d]);
+#endif
+        }
+    }
+    std::vector<int> ip(nleaf), np(nleaf);
+    for (int l = 0; l < nleaf; ++l) {
+        ip[l] = leaf[l + first_leaf].ipart;
+        np[l] = leaf[l + first_leaf].npart;
+    }
+    check("p2p_pass_begin", p2p_pass_begin(g_sess, n, pos.data(), nullptr, nleaf, ip.data(), np.data()));
+    g_pass_open = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time) {
+    const bool first_time = (g_call_cnt == 0);
+    g_tot_tasks += ntask;
+    g_call_cnt++;
+    P2PPack *pack = packlist;
+    pack->ntask = ntask;
+    pack->task_t = ltask_t;
+    pack->task_s = ltask_s;
+    pack->ileaf = first_leaf;
+    pack->nleaf = last_leaf - first_leaf;
+    pack->ipart = 0;
+    pack->npart = NPART;
+    pack->rankid = 0;
+    if (first_time) {
+        NPACK++;
+        begin_pass();
+    }
+    if (ntask > 0) {
+        // devMemcpyHD_task rebases the caller's arrays in place (src/gpu_func.impl.h:704-713)
+        for (int j = 0; j < ntask; ++j) {
+            ltask_t[j] -= first_leaf;
+            ltask_s[j] -= first_leaf;
+        }
+        check("p2p_pass_submit", p2p_pass_submit(g_sess, ntask, ltask_t, ltask_s));
+    }
+    if (last_time) {
+        g_tot_tasks = 0;
+        g_call_cnt = 0;
+    }
+    return NULL;
+}
+
+void *p2ppack_compute_gpu(P2PPack *packs, int npack) {
+    if (npack == 0) return NULL;
+    begin_pass();
+    for (int n = 0; n < npack; ++n) {
+        if (packs[n].ntask == 0) continue;
+        packs[n].rankid = 0;
+        std::vector<int> t(packs[n].ntask), s(packs[n].ntask);
+        for (int j = 0; j < packs[n].ntask; ++j) {
+            t[j] = packs[n].task_t[j] - first_leaf;
+            s[j] = packs[n].task_s[j] - first_leaf;
+        }
+        check("p2p_pass_submit", p2p_pass_submit(g_sess, packs[n].ntask, t.data(), s.data()));
+    }
+    return NULL;
+}
+
+void hostmalloc_task(int len) {
+    task_s = (int *)mymalloc(sizeof(int) * (size_t)len, 58);
+    task_t = (int *)mymalloc(sizeof(int) * (size_t)len, 59);
+}
+
+void hostrealloc_task(int len) {
+    task_s = (int *)myrealloc(task_s, sizeof(int) * (size_t)len, 58);
+    task_t = (int *)myrealloc(task_t, sizeof(int) * (size_t)len, 59);
+}
+
+void hostfree_task(void) {
+    myfree(task_s, 58);
+    myfree(task_t, 59);
+}
+
+double get_last_kntime(int proc_rank) {
+    (void)proc_rank;
+    if (!g_pass_open) return 0.0;
+    double sec = 0.0;
+    check("p2p_pass_end", p2p_pass_end(g_sess, &sec));
+    g_pass_open = false;
+    return sec;
+}
+
+void hostmalloc_out(int npart) {
+    g_out = (double *)malloc(sizeof(double) * 3 * (size_t)(npart > 0 ? npart : 1));
+    g_out_n = npart;
+}
+
+void hostfree_out(void) {
+    free(g_out);
+    g_out = nullptr;
+    g_out_n = 0;
+}
+
+// D2H of the result, then acc[d][j] += buf for the particles of each pack
+// (updateAcc_fromHostBuff, src/gpu_func.impl.h:644-681).
+void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
+    if (!g_sess) return;
+    bool any = false;
+    for (int n = 0; n < npack; ++n) any = any || packs[n].ntask != 0;
+    if (!any) return;
+    if (!g_out || g_out_n < NPART) {
+        fprintf(stderr, "devMemcpyDH_updateAcc: hostmalloc_out(%d) missing\n", NPART);
+        exit(EXIT_FAILURE);
+    }
+    check("p2p_pass_result", p2p_pass_result(g_sess, g_out));
+    const int n = NPART;
+    for (int p = 0; p < npack; ++p) {
+        if (packs[p].ntask == 0) continue;
+        for (int i = 0; i < packs[p].npart; ++i) {
+            const int j = packs[p].ipart + i;
+            if (active_level == -1 || (active_level && part[j].act == active_level)) {
+                acc[0][j] += g_out[j];
+                acc[1][j] += g_out[(size_t)n + j];
+                acc[2][j] += g_out[2 * (size_t)n + j];
+            }
+        }
+    }
+}
+
+void devfree(void) {
+    if (g_sess) p2p_session_destroy(g_sess);
+    g_sess = nullptr;
+    g_pass_open = false;
+    g_call_cnt = 0;
+    g_tot_tasks = 0;
+}
+
+void dinfofree(void) {}
+
+void sync_with_dev(void) {
+    if (g_sess) check("p2p_session_synchronize", p2p_session_synchronize(g_sess));
+}
+
+}  // extern "C"

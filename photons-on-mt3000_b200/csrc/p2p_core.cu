@@ -1,0 +1,836 @@
+// libphotons_p2p: host side of the B200 P2P pass and its C ABI
+// (include/photons_p2p.h). See p2p_kernels.cuh for the device code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "photons_p2p.h"
+#include "p2p_internal.h"
+#include "p2p_kernels.cuh"
+
+#define P2P_API extern "C" __attribute__((visibility("default")))
+
+namespace p2p {
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<int64_t> g_launches{0};
+
+int fail(int status, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return status;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t _e = (expr);                                                         \
+        if (_e != cudaSuccess)                                                           \
+            return fail(P2P_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                        __FILE__, __LINE__);                                             \
+    } while (0)
+
+#define P2P_TRY(expr)              \
+    do {                           \
+        int _s = (expr);           \
+        if (_s != P2P_OK) return _s; \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+// ----------------------------------------------------------- polynomial ---
+// H(u) = (1 - g(x)) / x^3 with x = sqrt(u), g(x) = erfc(x) + (2/sqrt(pi)) x e^{-x^2}.
+// The power series (4/sqrt(pi)) sum (-1)^n u^n / (n! (2n+3)) follows from
+// g'(x) = -(4/sqrt(pi)) x^2 e^{-x^2}; it is used near 0 where 1 - g cancels.
+double h_exact(double u) {
+    const double k = 4.0 / std::sqrt(M_PI);
+    if (u < 0.25) {
+        double term = 1.0, sum = 0.0;
+        for (int n = 0; n < 30; ++n) {
+            sum += term / (2 * n + 3);
+            term *= -u / (n + 1);
+        }
+        return k * sum;
+    }
+    const double x = std::sqrt(u);
+    const double g = std::erfc(x) + (2.0 / std::sqrt(M_PI)) * x * std::exp(-u);
+    return (1.0 - g) / (x * x * x);
+}
+
+struct PolyFit {
+    int degree = 0;
+    int ncoef_kernel = 0;  // template instance (degree + 1 rounded up)
+    double u0 = 0, umax = 0;
+    double max_err = 0;    // max over [0, umax] of sqrt(u) * |P(u) - H(u)|
+    float coef[kMaxCoef] = {0};
+};
+
+// Chebyshev interpolation of H on [0, umax] (nodes cos(pi (j + 1/2) / (D + 1))),
+// converted to monomials in t = u - u0 with u0 = umax / 2. The degree is the
+// smallest whose interpolation error, weighted by x (the pair force scales
+// as x * dH), stays below tol.
+PolyFit fit_h(double umax, double tol) {
+    static const int kDegrees[] = {8, 10, 12, 14, 16, 20};
+    PolyFit best;
+    const double half = 0.5 * umax;
+    for (int D : kDegrees) {
+        const int n = D + 1;
+        std::vector<double> fj(n), cheb(n);
+        for (int j = 0; j < n; ++j) {
+            const double tau = std::cos(M_PI * (j + 0.5) / n);
+            fj[j] = h_exact(half * (1.0 + tau));
+        }
+        for (int k = 0; k < n; ++k) {
+            double s = 0;
+            for (int j = 0; j < n; ++j) s += fj[j] * std::cos(M_PI * k * (j + 0.5) / n);
+            cheb[k] = (k == 0 ? 1.0 : 2.0) * s / n;
+        }
+        // Chebyshev series -> monomials in tau.
+        std::vector<double> mono(n, 0.0), tkm1(n, 0.0), tk(n, 0.0), tkp1(n, 0.0);
+        tkm1[0] = 1.0;  // T0
+        if (n > 1) tk[1] = 1.0;  // T1
+        for (int k = 0; k < n; ++k) {
+            const std::vector<double> &T = (k == 0) ? tkm1 : tk;
+            for (int m = 0; m < n; ++m) mono[m] += cheb[k] * T[m];
+            if (k >= 1) {
+                std::fill(tkp1.begin(), tkp1.end(), 0.0);
+                for (int m = 0; m + 1 < n; ++m) tkp1[m + 1] += 2.0 * tk[m];
+                for (int m = 0; m < n; ++m) tkp1[m] -= tkm1[m];
+                tkm1 = tk;
+                tk = tkp1;
+            }
+        }
+        // tau = t / half
+        std::vector<double> c(n);
+        double sc = 1.0;
+        for (int m = 0; m < n; ++m) {
+            c[m] = mono[m] / sc;
+            sc *= half;
+        }
+        double err = 0;
+        for (int q = 0; q <= 4000; ++q) {
+            const double u = umax * q / 4000.0;
+            const double t = u - half;
+            double h = c[n - 1];
+            for (int m = n - 2; m >= 0; --m) h = h * t + c[m];
+            err = std::max(err, std::sqrt(u) * std::fabs(h - h_exact(u)));
+        }
+        best.degree = D;
+        best.u0 = half;
+        best.umax = umax;
+        best.max_err = err;
+        std::memset(best.coef, 0, sizeof(best.coef));
+        for (int m = 0; m < n; ++m) best.coef[m] = (float)c[m];
+        best.ncoef_kernel = n;
+        if (err <= tol) break;
+    }
+    return best;
+}
+
+}  // namespace
+}  // namespace p2p
+
+using namespace p2p;
+
+struct p2p_session {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_k0 = nullptr, ev_k1 = nullptr;
+    bool kernel_timed = false;
+    p2p_params params{};
+    PolyFit fit;
+    // device buffers
+    DevBuf pos, mass, leaf_ip, leaf_np, task_t, task_s, meta, pos4, counts, fill, row_off,
+        row_src, tile_sums, acc, status, queue, pairs, probe;
+    // pass state
+    bool in_pass = false;
+    int npart = 0, nleaf = 0;
+    const double *d_pos = nullptr, *d_mass = nullptr;
+    const int *d_ip = nullptr, *d_np = nullptr;
+    // graph cache for p2p_pass_run_device
+    cudaGraphExec_t gexec = nullptr;
+    int graph_kernels = 0;
+    struct Key {
+        const void *p[6];
+        int64_t n[3];
+        int version;
+    } gkey{};
+    int version = 0;
+};
+
+namespace {
+
+int ensure(p2p_session *s, DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return P2P_OK;
+    size_t want = std::max(bytes + bytes / 4, (size_t)256);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (b.p) CUDA_TRY(cudaFree(b.p));
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return fail(P2P_ERR_NOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+    }
+    b.cap = want;
+    if (s->gexec) {  // cached graph refers to the old buffer
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    return P2P_OK;
+}
+
+bool is_fp32_form(int form) { return form != P2P_FORM_PLAIN_FP64; }
+
+int validate_params(const p2p_params *p) {
+    if (p->form < P2P_FORM_PLAIN_FP64 || p->form > P2P_FORM_KAHAN_FP32)
+        return fail(P2P_ERR_ARG, "unknown form %d", p->form);
+    if (p->soft_mode != P2P_SOFT_CLAMP && p->soft_mode != P2P_SOFT_PLUMMER)
+        return fail(P2P_ERR_ARG, "unknown soft_mode %d", p->soft_mode);
+    if (!(p->soften > 0.0) || !std::isfinite(p->soften))
+        return fail(P2P_ERR_ARG, "soften must be positive and finite");
+    if (!(p->split_radius > 0.0) || !std::isfinite(p->split_radius))
+        return fail(P2P_ERR_ARG, "split_radius must be positive and finite");
+    if (!std::isfinite(p->x_cut) || !std::isfinite(p->mass))
+        return fail(P2P_ERR_ARG, "x_cut and mass must be finite");
+    if (p->warps_per_block < 0 || p->warps_per_block > 8)
+        return fail(P2P_ERR_ARG, "warps_per_block must be in [0, 8]");
+    if (p->stage_sources < 0 || p->stage_sources > 2048 || (p->stage_sources % 32))
+        return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 2048]");
+    if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
+        return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
+    {
+        const int w = p->warps_per_block ? p->warps_per_block : 4;
+        const int st = p->stage_sources ? p->stage_sources : (p->form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
+        const size_t smem = (size_t)w * st * (p->form == P2P_FORM_PLAIN_FP64 ? 32 : 16);
+        if (smem > (size_t)227 * 1024)
+            return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
+    }
+    return P2P_OK;
+}
+
+int launch_count(int n) {
+    g_launches += n;
+    return P2P_OK;
+}
+
+struct Launch {
+    int warps, stage, blocks;
+    size_t smem;
+};
+
+Launch pair_launch_shape(const p2p_session *s) {
+    Launch L;
+    const bool fp64 = s->params.form == P2P_FORM_PLAIN_FP64;
+    L.warps = s->params.warps_per_block ? s->params.warps_per_block : 4;
+    L.stage = s->params.stage_sources ? s->params.stage_sources : (fp64 ? 128 : 256);
+    L.smem = (size_t)L.warps * L.stage * (fp64 ? sizeof(double4) : sizeof(float4));
+    int per_sm = s->params.blocks_per_sm;
+    if (!per_sm) {
+        // as many resident blocks as shared memory and 32 warps per SM allow
+        per_sm = std::max(1, std::min(32 / L.warps, (int)(200 * 1024 / std::max<size_t>(L.smem, 1))));
+    }
+    L.blocks = per_sm * s->sm_count;
+    return L;
+}
+
+template <int SOFT, bool MASSES, int ACC>
+int launch_split_nc(p2p_session *s, const PairArgs &a, const Launch &L) {
+    const int nc = s->fit.ncoef_kernel;
+#define P2P_NC_CASE(NCV)                                                                      \
+    case NCV: {                                                                               \
+        pair_split_kernel<SOFT, MASSES, ACC, NCV><<<L.blocks, L.warps * 32, L.smem, s->stream>>>( \
+            a, L.stage);                                                                      \
+        break;                                                                                \
+    }
+    switch (nc) {
+        P2P_NC_CASE(9)
+        P2P_NC_CASE(11)
+        P2P_NC_CASE(13)
+        P2P_NC_CASE(15)
+        P2P_NC_CASE(17)
+        P2P_NC_CASE(21)
+        default:
+            return fail(P2P_ERR_STATE, "no kernel for %d coefficients", nc);
+    }
+#undef P2P_NC_CASE
+    CUDA_TRY(cudaGetLastError());
+    return launch_count(1);
+}
+
+template <int SOFT, bool MASSES>
+int launch_split_acc(p2p_session *s, const PairArgs &a, const Launch &L) {
+    switch (s->params.form) {
+        case P2P_FORM_SPLIT:
+            return launch_split_nc<SOFT, MASSES, ACC_F64>(s, a, L);
+        case P2P_FORM_KAHAN_FP32:
+            return launch_split_nc<SOFT, MASSES, ACC_KAHAN>(s, a, L);
+        case P2P_FORM_NAIVE_FP32:
+            return launch_split_nc<SOFT, MASSES, ACC_F32>(s, a, L);
+        default:
+            return fail(P2P_ERR_STATE, "bad form");
+    }
+}
+
+template <int SOFT, bool MASSES>
+int launch_plain(p2p_session *s, const PairArgs &a, const Launch &L) {
+    pair_plain_kernel<SOFT, MASSES><<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage);
+    CUDA_TRY(cudaGetLastError());
+    return launch_count(1);
+}
+
+int launch_pair(p2p_session *s, const PairArgs &a) {
+    const Launch L = pair_launch_shape(s);
+    const bool masses = a.mass != nullptr;
+    const int soft = s->params.soft_mode;
+    if (s->params.form == P2P_FORM_PLAIN_FP64) {
+        if (soft == P2P_SOFT_CLAMP)
+            return masses ? launch_plain<SOFT_CLAMP, true>(s, a, L) : launch_plain<SOFT_CLAMP, false>(s, a, L);
+        return masses ? launch_plain<SOFT_PLUMMER, true>(s, a, L) : launch_plain<SOFT_PLUMMER, false>(s, a, L);
+    }
+    if (soft == P2P_SOFT_CLAMP)
+        return masses ? launch_split_acc<SOFT_CLAMP, true>(s, a, L) : launch_split_acc<SOFT_CLAMP, false>(s, a, L);
+    return masses ? launch_split_acc<SOFT_PLUMMER, true>(s, a, L) : launch_split_acc<SOFT_PLUMMER, false>(s, a, L);
+}
+
+// Opt every pair-kernel instance into the largest dynamic shared memory a
+// block may use (set once per device, outside any stream capture).
+constexpr int kMaxSmem = 227 * 1024;
+
+template <int SOFT, bool MASSES, int ACC>
+cudaError_t allow_smem_split() {
+    cudaError_t e = cudaSuccess;
+    const void *ks[] = {(const void *)pair_split_kernel<SOFT, MASSES, ACC, 9>,
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 11>,
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 13>,
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 15>,
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 17>,
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 21>};
+    for (const void *k : ks)
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    return e;
+}
+
+template <int SOFT, bool MASSES>
+cudaError_t allow_smem_soft() {
+    cudaError_t e = allow_smem_split<SOFT, MASSES, ACC_F64>();
+    if (e == cudaSuccess) e = allow_smem_split<SOFT, MASSES, ACC_KAHAN>();
+    if (e == cudaSuccess) e = allow_smem_split<SOFT, MASSES, ACC_F32>();
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void *)pair_plain_kernel<SOFT, MASSES>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    return e;
+}
+
+cudaError_t allow_smem_all() {
+    cudaError_t e = allow_smem_soft<SOFT_CLAMP, false>();
+    if (e == cudaSuccess) e = allow_smem_soft<SOFT_CLAMP, true>();
+    if (e == cudaSuccess) e = allow_smem_soft<SOFT_PLUMMER, false>();
+    if (e == cudaSuccess) e = allow_smem_soft<SOFT_PLUMMER, true>();
+    return e;
+}
+
+int grid_for(int64_t n, int threads, int cap_blocks) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap_blocks) b = cap_blocks;
+    return (int)b;
+}
+
+// Frame/coordinate preparation for the current pass inputs (stream-ordered).
+int enqueue_prep(p2p_session *s) {
+    const int nleaf = s->nleaf, npart = s->npart;
+    const int form = s->params.form;
+    LeafMeta *meta = (LeafMeta *)s->meta.p;
+    if (nleaf == 0) return P2P_OK;
+    const int threads = 256;
+    if (form == P2P_FORM_PLAIN_FP64) {
+        prep_plain_kernel<<<grid_for(nleaf, threads, 65535), threads, 0, s->stream>>>(
+            s->d_ip, s->d_np, npart, nleaf, meta, (int *)s->status.p);
+    } else {
+        const int blocks = grid_for((int64_t)nleaf * 32, threads, 65535);
+        const double c = 0.5 / s->params.split_radius;
+        if (form == P2P_FORM_NAIVE_FP32)
+            prep_split_kernel<false><<<blocks, threads, 0, s->stream>>>(
+                s->d_pos, s->d_mass, s->d_ip, s->d_np, npart, nleaf, c, meta, (float4 *)s->pos4.p,
+                (int *)s->status.p);
+        else
+            prep_split_kernel<true><<<blocks, threads, 0, s->stream>>>(
+                s->d_pos, s->d_mass, s->d_ip, s->d_np, npart, nleaf, c, meta, (float4 *)s->pos4.p,
+                (int *)s->status.p);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return launch_count(1);
+}
+
+PairArgs make_args(p2p_session *s) {
+    PairArgs a;
+    std::memset(&a, 0, sizeof(a));
+    const p2p_params &p = s->params;
+    a.leaf = (const LeafMeta *)s->meta.p;
+    a.row_off = (const int64_t *)s->row_off.p;
+    a.row_src = (const int *)s->row_src.p;
+    a.pos4 = (const float4 *)s->pos4.p;
+    a.pos = s->d_pos;
+    a.mass = s->d_mass;
+    a.acc = (double *)s->acc.p;
+    a.queue = (int *)s->queue.p;
+    a.npart = s->npart;
+    a.nleaf = s->nleaf;
+    const double c = 0.5 / p.split_radius;
+    a.cscale = c;
+    a.eps2 = (float)((c * p.soften) * (c * p.soften));
+    a.u0 = (float)s->fit.u0;
+    a.ucut = (float)s->fit.umax;
+    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = s->fit.coef[k];
+    a.out_scale = c * c * (s->d_mass ? 1.0 : p.mass);
+    a.soft = p.soften;
+    a.r_soft = 1.0 / p.soften;
+    a.rrs = 1.0 / p.split_radius;
+    a.hrrs = 0.5 * a.rrs;
+    a.coeff = 2.0 * (1.0 / std::sqrt(M_PI));
+    a.xcut = p.x_cut;
+    a.mass_eq = p.mass;
+    return a;
+}
+
+// CSR build + pair kernel for one list chunk already on the device.
+int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed) {
+    if (ntask <= 0 || s->nleaf <= 0) return P2P_OK;
+    const int nleaf = s->nleaf;
+    const int threads = 256;
+    CUDA_TRY(cudaMemsetAsync(s->counts.p, 0, sizeof(int) * (size_t)nleaf, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->fill.p, 0, sizeof(int) * (size_t)nleaf, s->stream));
+    const int eblocks = grid_for(ntask, threads, 148 * 16);
+    csr_count_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf,
+                                                         (const LeafMeta *)s->meta.p,
+                                                         (int *)s->counts.p,
+                                                         (unsigned long long *)s->pairs.p,
+                                                         (int *)s->status.p);
+    CUDA_TRY(cudaGetLastError());
+    const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
+    int64_t *row_off = (int64_t *)s->row_off.p;
+    int64_t *tiles = (int64_t *)s->tile_sums.p;
+    scan_tiles_kernel<<<ntiles, kScanThreads, 0, s->stream>>>((const int *)s->counts.p, nleaf,
+                                                              row_off, tiles);
+    scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>(tiles, ntiles, row_off + nleaf);
+    scan_add_kernel<<<grid_for(nleaf, threads, 1 << 30), threads, 0, s->stream>>>(row_off, nleaf,
+                                                                                  tiles);
+    CUDA_TRY(cudaGetLastError());
+    csr_scatter_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf, row_off,
+                                                           (int *)s->fill.p, (int *)s->row_src.p);
+    CUDA_TRY(cudaGetLastError());
+    launch_count(5);
+    CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
+    PairArgs a = make_args(s);
+    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k0, s->stream, cudaEventRecordExternal));
+    P2P_TRY(launch_pair(s, a));
+    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k1, s->stream, cudaEventRecordExternal));
+    s->kernel_timed = timed;
+    return P2P_OK;
+}
+
+int size_pass_buffers(p2p_session *s, int npart, int nleaf, bool host_inputs, bool masses) {
+    const size_t n3 = 3 * (size_t)npart;
+    if (host_inputs) {
+        P2P_TRY(ensure(s, s->pos, sizeof(double) * n3));
+        if (masses) P2P_TRY(ensure(s, s->mass, sizeof(double) * (size_t)npart));
+        P2P_TRY(ensure(s, s->leaf_ip, sizeof(int) * (size_t)nleaf));
+        P2P_TRY(ensure(s, s->leaf_np, sizeof(int) * (size_t)nleaf));
+    }
+    P2P_TRY(ensure(s, s->acc, sizeof(double) * n3));
+    P2P_TRY(ensure(s, s->meta, sizeof(LeafMeta) * (size_t)nleaf));
+    if (is_fp32_form(s->params.form)) P2P_TRY(ensure(s, s->pos4, sizeof(float4) * (size_t)npart));
+    P2P_TRY(ensure(s, s->counts, sizeof(int) * (size_t)nleaf));
+    P2P_TRY(ensure(s, s->fill, sizeof(int) * (size_t)nleaf));
+    P2P_TRY(ensure(s, s->row_off, sizeof(int64_t) * ((size_t)nleaf + 1)));
+    const size_t ntiles = ((size_t)nleaf + kScanTile - 1) / kScanTile + 1;
+    P2P_TRY(ensure(s, s->tile_sums, sizeof(int64_t) * ntiles));
+    P2P_TRY(ensure(s, s->status, sizeof(int)));
+    P2P_TRY(ensure(s, s->queue, sizeof(int)));
+    P2P_TRY(ensure(s, s->pairs, sizeof(unsigned long long)));
+    return P2P_OK;
+}
+
+int begin_common(p2p_session *s) {
+    CUDA_TRY(cudaMemsetAsync(s->acc.p, 0, sizeof(double) * 3 * (size_t)s->npart, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->pairs.p, 0, sizeof(unsigned long long), s->stream));
+    return enqueue_prep(s);
+}
+
+int check_session(p2p_session *s) {
+    if (!s) return fail(P2P_ERR_ARG, "null session");
+    CUDA_TRY(cudaSetDevice(s->device));
+    return P2P_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ ABI ---
+
+P2P_API void p2p_params_default(p2p_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->form = P2P_FORM_PLAIN_FP64;
+    p->soft_mode = P2P_SOFT_CLAMP;
+    p->soften = 1.0;
+    p->split_radius = 1.0;
+    p->x_cut = 2.8125;
+    p->mass = 1.0;
+}
+
+P2P_API const char *p2p_status_string(int status) {
+    switch (status) {
+        case P2P_OK: return "ok";
+        case P2P_ERR_ARG: return "invalid argument";
+        case P2P_ERR_CUDA: return "CUDA error";
+        case P2P_ERR_STATE: return "call out of order";
+        case P2P_ERR_NOMEM: return "out of device memory";
+        case P2P_ERR_RANGE: return "input index out of range";
+        case P2P_ERR_CAPACITY: return "input exceeds fixed capacity";
+        default: return "unknown status";
+    }
+}
+
+P2P_API const char *p2p_last_error(void) { return g_last_error.c_str(); }
+
+P2P_API int p2p_version(void) { return 10000; }
+
+P2P_API int p2p_device_count(int *count) {
+    if (!count) return fail(P2P_ERR_ARG, "null argument");
+    *count = 0;
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *count = 0;
+        if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return P2P_OK;
+        return fail(P2P_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    return P2P_OK;
+}
+
+P2P_API int p2p_session_create(int device, p2p_session **out) {
+    if (!out) return fail(P2P_ERR_ARG, "null out");
+    *out = nullptr;
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(P2P_ERR_ARG, "device %d of %d", device, ndev);
+    CUDA_TRY(cudaSetDevice(device));
+    p2p_session *s = new p2p_session();
+    s->device = device;
+    cudaError_t e = cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_begin);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_end);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_k0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_k1);
+    if (e == cudaSuccess) e = allow_smem_all();
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(P2P_ERR_CUDA, "session setup: %s", cudaGetErrorString(e));
+    }
+    p2p_params_default(&s->params);
+    *out = s;
+    return P2P_OK;
+}
+
+P2P_API int p2p_session_destroy(p2p_session *s) {
+    if (!s) return P2P_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    DevBuf *bufs[] = {&s->pos, &s->mass, &s->leaf_ip, &s->leaf_np, &s->task_t, &s->task_s,
+                      &s->meta, &s->pos4, &s->counts, &s->fill, &s->row_off, &s->row_src,
+                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->probe};
+    for (DevBuf *b : bufs)
+        if (b->p) cudaFree(b->p);
+    cudaEvent_t evs[] = {s->ev_begin, s->ev_end, s->ev_k0, s->ev_k1};
+    for (cudaEvent_t ev : evs)
+        if (ev) cudaEventDestroy(ev);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return P2P_OK;
+}
+
+P2P_API int p2p_session_set_params(p2p_session *s, const p2p_params *params) {
+    if (!s || !params) return fail(P2P_ERR_ARG, "null argument");
+    if (s->in_pass) return fail(P2P_ERR_STATE, "cannot change parameters inside a pass");
+    P2P_TRY(validate_params(params));
+    s->params = *params;
+    if (is_fp32_form(params->form)) {
+        const double xmax = params->x_cut > 0.0 ? params->x_cut : 4.0;
+        s->fit = fit_h(xmax * xmax, 2e-8);
+    } else {
+        s->fit = PolyFit();
+    }
+    s->version++;
+    if (s->gexec) {
+        cudaGraphExecDestroy(s->gexec);
+        s->gexec = nullptr;
+    }
+    return P2P_OK;
+}
+
+P2P_API int p2p_session_get_params(const p2p_session *s, p2p_params *params) {
+    if (!s || !params) return fail(P2P_ERR_ARG, "null argument");
+    *params = s->params;
+    return P2P_OK;
+}
+
+P2P_API void *p2p_session_stream(p2p_session *s) { return s ? (void *)s->stream : nullptr; }
+
+P2P_API int p2p_session_poly_degree(const p2p_session *s) { return s ? s->fit.degree : 0; }
+
+P2P_API double p2p_session_poly_error(const p2p_session *s) { return s ? s->fit.max_err : 0.0; }
+
+P2P_API int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *masses,
+                           int nleaf, const int *leaf_ipart, const int *leaf_npart) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass already open");
+    if (npart < 0 || nleaf < 0) return fail(P2P_ERR_ARG, "negative size");
+    if ((npart > 0 && !pos) || (nleaf > 0 && (!leaf_ipart || !leaf_npart)))
+        return fail(P2P_ERR_ARG, "null input");
+    for (int l = 0; l < nleaf; ++l) {
+        const int64_t ip = leaf_ipart[l], np = leaf_npart[l];
+        if (ip < 0 || np < 0 || ip + np > npart)
+            return fail(P2P_ERR_RANGE, "leaf %d covers [%lld, %lld) outside [0, %d)", l,
+                        (long long)ip, (long long)(ip + np), npart);
+    }
+    P2P_TRY(size_pass_buffers(s, npart, nleaf, true, masses != nullptr));
+    s->npart = npart;
+    s->nleaf = nleaf;
+    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
+    if (npart) CUDA_TRY(cudaMemcpyAsync(s->pos.p, pos, sizeof(double) * 3 * (size_t)npart, cudaMemcpyHostToDevice, s->stream));
+    if (masses && npart)
+        CUDA_TRY(cudaMemcpyAsync(s->mass.p, masses, sizeof(double) * (size_t)npart, cudaMemcpyHostToDevice, s->stream));
+    if (nleaf) {
+        CUDA_TRY(cudaMemcpyAsync(s->leaf_ip.p, leaf_ipart, sizeof(int) * (size_t)nleaf, cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(s->leaf_np.p, leaf_npart, sizeof(int) * (size_t)nleaf, cudaMemcpyHostToDevice, s->stream));
+    }
+    s->d_pos = (const double *)s->pos.p;
+    s->d_mass = masses ? (const double *)s->mass.p : nullptr;
+    s->d_ip = (const int *)s->leaf_ip.p;
+    s->d_np = (const int *)s->leaf_np.p;
+    P2P_TRY(begin_common(s));
+    s->in_pass = true;
+    s->kernel_timed = false;
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_begin_device(p2p_session *s, int npart, const double *d_pos,
+                                  const double *d_masses, int nleaf, const int *d_leaf_ipart,
+                                  const int *d_leaf_npart) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass already open");
+    if (npart < 0 || nleaf < 0) return fail(P2P_ERR_ARG, "negative size");
+    if ((npart > 0 && !d_pos) || (nleaf > 0 && (!d_leaf_ipart || !d_leaf_npart)))
+        return fail(P2P_ERR_ARG, "null input");
+    P2P_TRY(size_pass_buffers(s, npart, nleaf, false, false));
+    s->npart = npart;
+    s->nleaf = nleaf;
+    s->d_pos = d_pos;
+    s->d_mass = d_masses;
+    s->d_ip = d_leaf_ipart;
+    s->d_np = d_leaf_npart;
+    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
+    P2P_TRY(begin_common(s));
+    s->in_pass = true;
+    s->kernel_timed = false;
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, const int *task_s) {
+    P2P_TRY(check_session(s));
+    if (!s->in_pass) return fail(P2P_ERR_STATE, "no open pass");
+    if (ntask < 0) return fail(P2P_ERR_ARG, "negative ntask");
+    if (ntask == 0) return P2P_OK;
+    if (!task_t || !task_s) return fail(P2P_ERR_ARG, "null task list");
+    P2P_TRY(ensure(s, s->task_t, sizeof(int) * (size_t)ntask));
+    P2P_TRY(ensure(s, s->task_s, sizeof(int) * (size_t)ntask));
+    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)ntask));
+    CUDA_TRY(cudaMemcpyAsync(s->task_t.p, task_t, sizeof(int) * (size_t)ntask, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(s->task_s.p, task_s, sizeof(int) * (size_t)ntask, cudaMemcpyHostToDevice, s->stream));
+    return enqueue_chunk(s, ntask, (const int *)s->task_t.p, (const int *)s->task_s.p, true);
+}
+
+P2P_API int p2p_pass_submit_device(p2p_session *s, int64_t ntask, const int *d_task_t,
+                                   const int *d_task_s) {
+    P2P_TRY(check_session(s));
+    if (!s->in_pass) return fail(P2P_ERR_STATE, "no open pass");
+    if (ntask < 0) return fail(P2P_ERR_ARG, "negative ntask");
+    if (ntask == 0) return P2P_OK;
+    if (!d_task_t || !d_task_s) return fail(P2P_ERR_ARG, "null task list");
+    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)ntask));
+    return enqueue_chunk(s, ntask, d_task_t, d_task_s, true);
+}
+
+P2P_API int p2p_pass_end(p2p_session *s, double *gpu_seconds) {
+    P2P_TRY(check_session(s));
+    if (!s->in_pass) return fail(P2P_ERR_STATE, "no open pass");
+    s->in_pass = false;
+    CUDA_TRY(cudaEventRecord(s->ev_end, s->stream));
+    CUDA_TRY(cudaEventSynchronize(s->ev_end));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_begin, s->ev_end));
+    if (gpu_seconds) *gpu_seconds = ms * 1e-3;
+    int status = 0;
+    CUDA_TRY(cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status & ST_LEAF_RANGE) return fail(P2P_ERR_RANGE, "a leaf range lies outside the particles");
+    if (status & ST_TASK_RANGE) return fail(P2P_ERR_RANGE, "a task entry names a leaf outside [0, nleaf)");
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_accumulate(p2p_session *s, double *acc) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass still open; call p2p_pass_end first");
+    if (!acc && s->npart) return fail(P2P_ERR_ARG, "null acc");
+    const size_t n3 = 3 * (size_t)s->npart;
+    std::vector<double> buf(n3);
+    if (n3) CUDA_TRY(cudaMemcpy(buf.data(), s->acc.p, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n3; ++i) acc[i] += buf[i];
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_result(p2p_session *s, double *out) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass still open; call p2p_pass_end first");
+    if (!out && s->npart) return fail(P2P_ERR_ARG, "null out");
+    const size_t n3 = 3 * (size_t)s->npart;
+    if (n3) CUDA_TRY(cudaMemcpy(out, s->acc.p, sizeof(double) * n3, cudaMemcpyDeviceToHost));
+    return P2P_OK;
+}
+
+P2P_API int p2p_session_synchronize(p2p_session *s) {
+    P2P_TRY(check_session(s));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_result_device(p2p_session *s, const double **d_acc) {
+    if (!s || !d_acc) return fail(P2P_ERR_ARG, "null argument");
+    *d_acc = (const double *)s->acc.p;
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_pair_count(p2p_session *s, int64_t *pairs) {
+    P2P_TRY(check_session(s));
+    if (!pairs) return fail(P2P_ERR_ARG, "null argument");
+    unsigned long long v = 0;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(cudaMemcpy(&v, s->pairs.p, sizeof(v), cudaMemcpyDeviceToHost));
+    *pairs = (int64_t)v;
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_run_device(p2p_session *s, int npart, const double *d_pos,
+                                const double *d_masses, int nleaf, const int *d_leaf_ipart,
+                                const int *d_leaf_npart, int64_t ntask, const int *d_task_t,
+                                const int *d_task_s) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass already open");
+    if (npart < 0 || nleaf < 0 || ntask < 0) return fail(P2P_ERR_ARG, "negative size");
+    if ((npart > 0 && !d_pos) || (nleaf > 0 && (!d_leaf_ipart || !d_leaf_npart)) ||
+        (ntask > 0 && (!d_task_t || !d_task_s)))
+        return fail(P2P_ERR_ARG, "null input");
+    p2p_session::Key key{};
+    key.p[0] = d_pos; key.p[1] = d_masses; key.p[2] = d_leaf_ipart; key.p[3] = d_leaf_npart;
+    key.p[4] = d_task_t; key.p[5] = d_task_s;
+    key.n[0] = npart; key.n[1] = nleaf; key.n[2] = ntask;
+    key.version = s->version;
+    // sizing may drop a cached graph (buffers moved)
+    P2P_TRY(size_pass_buffers(s, npart, nleaf, false, false));
+    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)std::max<int64_t>(ntask, 1)));
+    s->npart = npart;
+    s->nleaf = nleaf;
+    s->d_pos = d_pos;
+    s->d_mass = d_masses;
+    s->d_ip = d_leaf_ipart;
+    s->d_np = d_leaf_npart;
+    const bool hit = s->gexec && std::memcmp(&key, &s->gkey, sizeof(key)) == 0;
+    if (!hit) {
+        if (s->gexec) {
+            cudaGraphExecDestroy(s->gexec);
+            s->gexec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t before = g_launches.load();
+        int st = begin_common(s);
+        if (st == P2P_OK) st = enqueue_chunk(s, ntask, d_task_t, d_task_s, true);
+        cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
+        const int64_t captured = g_launches.load() - before;
+        g_launches -= captured;  // capture does not launch; replays are counted below
+        if (st != P2P_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ce != cudaSuccess) return fail(P2P_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        cudaError_t ie = cudaGraphInstantiate(&s->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            s->gexec = nullptr;
+            return fail(P2P_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ie));
+        }
+        s->graph_kernels = (int)captured;
+        s->gkey = key;
+    }
+    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
+    CUDA_TRY(cudaGraphLaunch(s->gexec, s->stream));
+    g_launches += s->graph_kernels;
+    s->kernel_timed = ntask > 0 && nleaf > 0;
+    s->in_pass = true;
+    return P2P_OK;
+}
+
+P2P_API int64_t p2p_kernel_launch_count(void) { return g_launches.load(); }
+
+P2P_API int p2p_session_last_kernel_ms(p2p_session *s, float *ms) {
+    if (!s || !ms) return fail(P2P_ERR_ARG, "null argument");
+    *ms = 0.f;
+    if (!s->kernel_timed) return P2P_OK;
+    CUDA_TRY(cudaEventSynchronize(s->ev_k1));
+    CUDA_TRY(cudaEventElapsedTime(ms, s->ev_k0, s->ev_k1));
+    return P2P_OK;
+}
+
+P2P_API int p2p_measure_fp32_peak(p2p_session *s, double *tflops) {
+    P2P_TRY(check_session(s));
+    if (!tflops) return fail(P2P_ERR_ARG, "null argument");
+    const int threads = 256, blocks = s->sm_count * 8, iters = 4096;
+    P2P_TRY(ensure(s, s->probe, sizeof(float) * (size_t)threads * blocks));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        CUDA_TRY(cudaEventRecord(s->ev_k0, s->stream));
+        fma_probe_kernel<<<blocks, threads, 0, s->stream>>>((float *)s->probe.p, iters, 0.9999999f, 1e-7f);
+        CUDA_TRY(cudaGetLastError());
+        launch_count(1);
+        CUDA_TRY(cudaEventRecord(s->ev_k1, s->stream));
+        CUDA_TRY(cudaEventSynchronize(s->ev_k1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_k0, s->ev_k1));
+        best = std::min(best, ms);
+    }
+    const double flops = 2.0 * 8 * 8 * (double)iters * threads * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    s->kernel_timed = false;
+    return P2P_OK;
+}

@@ -1,0 +1,47 @@
+// Internal definitions shared by the host and device code of libphotons_p2p.
+#pragma once
+
+#include <cstdint>
+
+namespace p2p {
+
+// Per-leaf record the pair kernels read for every source entry: the FP64
+// frame centre the leaf's FP32 coordinates are relative to, and its particle
+// range. 32 bytes, one 32 B sector per lookup.
+struct __align__(16) LeafMeta {
+    double cx, cy, cz;
+    int ipart, npart;
+};
+
+// Status bits the device sets instead of faulting on bad input.
+enum : int {
+    ST_LEAF_RANGE = 1,  // a leaf's particle range lies outside [0, npart)
+    ST_TASK_RANGE = 2,  // a task entry names a leaf outside [0, nleaf)
+};
+
+constexpr int kMaxCoef = 21;  // polynomial degree <= 20
+
+// Arguments of the pair kernels, passed by value (constant bank).
+struct PairArgs {
+    const LeafMeta *leaf;
+    const int64_t *row_off;  // nleaf + 1
+    const int *row_src;      // source leaf ids, grouped by sink row
+    const float4 *pos4;      // FP32 forms: (x', y', z', w) in the leaf frame, scaled by c
+    const double *pos;       // FP64 form: SoA positions
+    const double *mass;      // FP64 form: per-particle masses or null
+    double *acc;             // SoA 3 * npart, +=
+    int *queue;              // persistent work counter (reset to 0 before launch)
+    int npart, nleaf;
+    // FP32 forms (scaled units: lengths times c = 1 / (2 r_s))
+    float eps2;              // (c * eps)^2
+    float u0;                // polynomial expansion point
+    float ucut;              // x_cut^2 (or the fitted domain end without cutoff)
+    float pad0;
+    double cscale;           // c
+    double out_scale;        // c^2 * mass (equal masses) or c^2 (per-particle masses)
+    float coef[kMaxCoef];    // H(u) ~ sum coef[k] (u - u0)^k
+    // FP64 form (reference units)
+    double soft, r_soft, hrrs, rrs, coeff, xcut, mass_eq;
+};
+
+}  // namespace p2p

@@ -1,0 +1,569 @@
+// Device code of the P2P pass for sm_100a.
+//
+// Pass structure on the device (one chunk of the interaction list):
+//   prep        one warp per leaf: FP64 frame centre (bounding-box midpoint of
+//               the leaf's particles) and FP32 coordinates relative to it,
+//               scaled by c = 1/(2 r_s); the FP64 form keeps FP64 positions.
+//   csr_count   sink histogram of the (sink, source) list + pair count
+//   scan        exclusive scan of the histogram -> row offsets (int64)
+//   csr_scatter sources grouped by sink row
+//   pair kernel persistent, one warp per sink row taken from an atomic work
+//               counter; the row's source leaves are staged in shared memory
+//               in the sink's frame, every lane owns a sink particle (or a
+//               share of one, for rows with <= 16 sink particles) and streams
+//               the staged sources.
+//
+// The reference builds the same CSR with thrust::sort_by_key /
+// reduce_by_key / exclusive_scan (src/gpu_entry.cu:132-138) and runs
+// P2P_kernel3 with one CTA per sink leaf (src/gpu_kernel.impl.h:439-524).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "p2p_internal.h"
+
+namespace p2p {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// ---------------------------------------------------------------- prep ----
+
+// FP32 forms: frame centres and scaled FP32 coordinates. LOCAL = false puts
+// every leaf's frame at the origin (global FP32 coordinates, the naive form).
+template <bool LOCAL>
+__global__ void prep_split_kernel(const double *__restrict__ pos, const double *__restrict__ mass,
+                                  const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
+                                  int npart, int nleaf, double cscale, LeafMeta *__restrict__ meta,
+                                  float4 *__restrict__ pos4, int *__restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; l < nleaf; l += nwarps) {
+        const int ip = leaf_ip[l], np = leaf_np[l];
+        const bool ok = ip >= 0 && np >= 0 && (int64_t)ip + np <= npart;
+        if (!ok) {
+            if (lane == 0) {
+                atomicOr(status, ST_LEAF_RANGE);
+                LeafMeta m;
+                m.cx = m.cy = m.cz = 0.0;
+                m.ipart = 0;
+                m.npart = 0;
+                meta[l] = m;
+            }
+            continue;
+        }
+        const double *X = pos, *Y = pos + npart, *Z = pos + 2 * (size_t)npart;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        if (LOCAL && np > 0) {
+            double lo0 = 1e300, lo1 = 1e300, lo2 = 1e300, hi0 = -1e300, hi1 = -1e300, hi2 = -1e300;
+            for (int q = lane; q < np; q += 32) {
+                const double x = X[ip + q], y = Y[ip + q], z = Z[ip + q];
+                lo0 = fmin(lo0, x); hi0 = fmax(hi0, x);
+                lo1 = fmin(lo1, y); hi1 = fmax(hi1, y);
+                lo2 = fmin(lo2, z); hi2 = fmax(hi2, z);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                lo0 = fmin(lo0, __shfl_xor_sync(kFull, lo0, off));
+                lo1 = fmin(lo1, __shfl_xor_sync(kFull, lo1, off));
+                lo2 = fmin(lo2, __shfl_xor_sync(kFull, lo2, off));
+                hi0 = fmax(hi0, __shfl_xor_sync(kFull, hi0, off));
+                hi1 = fmax(hi1, __shfl_xor_sync(kFull, hi1, off));
+                hi2 = fmax(hi2, __shfl_xor_sync(kFull, hi2, off));
+            }
+            c0 = 0.5 * (lo0 + hi0);
+            c1 = 0.5 * (lo1 + hi1);
+            c2 = 0.5 * (lo2 + hi2);
+        }
+        if (lane == 0) {
+            LeafMeta m;
+            m.cx = c0;
+            m.cy = c1;
+            m.cz = c2;
+            m.ipart = ip;
+            m.npart = np;
+            meta[l] = m;
+        }
+        for (int q = lane; q < np; q += 32) {
+            const int i = ip + q;
+            pos4[i] = make_float4((float)((X[i] - c0) * cscale), (float)((Y[i] - c1) * cscale),
+                                  (float)((Z[i] - c2) * cscale), mass ? (float)mass[i] : 1.0f);
+        }
+    }
+}
+
+// FP64 form: leaf table only (positions stay FP64 SoA).
+__global__ void prep_plain_kernel(const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
+                                  int npart, int nleaf, LeafMeta *__restrict__ meta,
+                                  int *__restrict__ status) {
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaf; l += gridDim.x * blockDim.x) {
+        int ip = leaf_ip[l], np = leaf_np[l];
+        if (!(ip >= 0 && np >= 0 && (int64_t)ip + np <= npart)) {
+            atomicOr(status, ST_LEAF_RANGE);
+            ip = 0;
+            np = 0;
+        }
+        LeafMeta m;
+        m.cx = m.cy = m.cz = 0.0;
+        m.ipart = ip;
+        m.npart = np;
+        meta[l] = m;
+    }
+}
+
+// ----------------------------------------------------------------- CSR ----
+
+__global__ void csr_count_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
+                                 int nleaf, const LeafMeta *__restrict__ meta,
+                                 int *__restrict__ counts, unsigned long long *__restrict__ pairs,
+                                 int *__restrict__ status) {
+    __shared__ unsigned long long block_pairs;
+    if (threadIdx.x == 0) block_pairs = 0;
+    __syncthreads();
+    unsigned long long local = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        const int t = tt[e], s = ts[e];
+        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) {
+            atomicOr(status, ST_TASK_RANGE);
+            continue;
+        }
+        atomicAdd(&counts[t], 1);
+        local += (unsigned long long)meta[t].npart * (unsigned long long)meta[s].npart;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(kFull, local, off);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(&block_pairs, local);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_pairs) atomicAdd(pairs, block_pairs);
+}
+
+__global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
+                                   int nleaf, const int64_t *__restrict__ row_off,
+                                   int *__restrict__ fill, int *__restrict__ row_src) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        const int t = tt[e], s = ts[e];
+        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) continue;
+        const int k = atomicAdd(&fill[t], 1);
+        row_src[row_off[t] + k] = s;
+    }
+}
+
+// Exclusive scan int32 -> int64 in three kernels. kScanTile elements per block.
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t *warp_sums,
+                                                        int64_t *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int64_t y = __shfl_up_sync(kFull, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t ws = lane < (kScanThreads / 32) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int64_t y = __shfl_up_sync(kFull, ws, off);
+            if (lane >= off) ws += y;
+        }
+        if (lane < (kScanThreads / 32)) warp_sums[lane] = ws;
+    }
+    __syncthreads();
+    const int64_t before = (w > 0 ? warp_sums[w - 1] : 0) + x - v;
+    if (total) *total = warp_sums[kScanThreads / 32 - 1];
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_tiles_kernel(const int *__restrict__ in, int n, int64_t *__restrict__ out,
+                  int64_t *__restrict__ tile_sums) {
+    __shared__ int64_t warp_sums[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
+    int64_t v[kScanPer];
+    int64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        s += v[k];
+    }
+    int64_t total;
+    int64_t run = block_exclusive_scan(s, warp_sums, &total);
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_sums_kernel(int64_t *__restrict__ tile_sums, int ntiles, int64_t *__restrict__ grand_total) {
+    __shared__ int64_t warp_sums[kScanThreads / 32];
+    int64_t carry = 0;
+    for (int b0 = 0; b0 < ntiles; b0 += kScanThreads) {
+        const int i = b0 + threadIdx.x;
+        const int64_t v = i < ntiles ? tile_sums[i] : 0;
+        int64_t total;
+        const int64_t ex = block_exclusive_scan(v, warp_sums, &total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grand_total = carry;
+}
+
+__global__ void scan_add_kernel(int64_t *__restrict__ out, int n,
+                                const int64_t *__restrict__ tile_sums) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_sums[i / kScanTile];
+}
+
+// ------------------------------------------------------------ pair: FP32 ---
+
+enum { ACC_F64 = 0, ACC_KAHAN = 1, ACC_F32 = 2 };
+enum { SOFT_CLAMP = 0, SOFT_PLUMMER = 1 };
+
+struct AccF64 {
+    double x = 0.0, y = 0.0, z = 0.0;
+    __device__ __forceinline__ void add(float ax, float ay, float az) {
+        x += (double)ax;
+        y += (double)ay;
+        z += (double)az;
+    }
+    __device__ __forceinline__ void reduce_xor(int from) {
+        for (int off = from; off < 32; off <<= 1) {
+            x += __shfl_xor_sync(kFull, x, off);
+            y += __shfl_xor_sync(kFull, y, off);
+            z += __shfl_xor_sync(kFull, z, off);
+        }
+    }
+    __device__ __forceinline__ double vx() const { return x; }
+    __device__ __forceinline__ double vy() const { return y; }
+    __device__ __forceinline__ double vz() const { return z; }
+};
+
+struct AccKahan {
+    float x = 0.f, y = 0.f, z = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    __device__ __forceinline__ static void kadd(float &s, float &c, float v) {
+        const float yv = v - c;
+        const float t = s + yv;
+        c = (t - s) - yv;
+        s = t;
+    }
+    __device__ __forceinline__ void add(float ax, float ay, float az) {
+        kadd(x, cx, ax);
+        kadd(y, cy, ay);
+        kadd(z, cz, az);
+    }
+    __device__ __forceinline__ void reduce_xor(int from) {
+        x -= cx; y -= cy; z -= cz;
+        cx = cy = cz = 0.f;
+        for (int off = from; off < 32; off <<= 1) {
+            x += __shfl_xor_sync(kFull, x, off);
+            y += __shfl_xor_sync(kFull, y, off);
+            z += __shfl_xor_sync(kFull, z, off);
+        }
+    }
+    __device__ __forceinline__ double vx() const { return x; }
+    __device__ __forceinline__ double vy() const { return y; }
+    __device__ __forceinline__ double vz() const { return z; }
+};
+
+struct AccF32 {
+    float x = 0.f, y = 0.f, z = 0.f;
+    __device__ __forceinline__ void add(float ax, float ay, float az) {
+        x += ax;
+        y += ay;
+        z += az;
+    }
+    __device__ __forceinline__ void reduce_xor(int from) {
+        for (int off = from; off < 32; off <<= 1) {
+            x += __shfl_xor_sync(kFull, x, off);
+            y += __shfl_xor_sync(kFull, y, off);
+            z += __shfl_xor_sync(kFull, z, off);
+        }
+    }
+    __device__ __forceinline__ double vx() const { return x; }
+    __device__ __forceinline__ double vy() const { return y; }
+    __device__ __forceinline__ double vz() const { return z; }
+};
+
+template <int ACC> struct AccSel;
+template <> struct AccSel<ACC_F64> { using T = AccF64; };
+template <> struct AccSel<ACC_KAHAN> { using T = AccKahan; };
+template <> struct AccSel<ACC_F32> { using T = AccF32; };
+
+// One pair in scaled units (lengths times c = 1/(2 r_s)). With u = x^2 the
+// squared (softened) separation, the truncated kernel
+//     g(x) / r^3,   g(x) = erfc(x) + (2/sqrt(pi)) x exp(-x^2)
+// is written as g(x) = 1 - x^3 H(x^2), so that in scaled units
+//     f = rinv^3 - H(u),   H(u) = sum coef[k] (u - u0)^k,
+// a polynomial directly in u: one MUFU rsqrt, no exp, no divide.
+template <int SOFT, bool MASSES, int NC>
+__device__ __forceinline__ void pair_split(const float4 s, const float px, const float py,
+                                           const float pz, const PairArgs &a, float &ax, float &ay,
+                                           float &az) {
+    const float dx = s.x - px, dy = s.y - py, dz = s.z - pz;
+    float u;
+    if (SOFT == SOFT_PLUMMER) {
+        u = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, a.eps2)));
+    } else {
+        u = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), a.eps2);
+    }
+    const float rinv = rsqrt_approx(u);
+    const float rinv3 = rinv * rinv * rinv;
+    const float t = u - a.u0;
+    float h = a.coef[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) h = fmaf(h, t, a.coef[k]);
+    float f = rinv3 - h;
+    f = (u <= a.ucut) ? f : 0.0f;
+    if (MASSES) f *= s.w;
+    ax = fmaf(dx, f, ax);
+    ay = fmaf(dy, f, ay);
+    az = fmaf(dz, f, az);
+}
+
+// Staged sources are consumed in FP32 partial sums of at most kFlush
+// sources per lane before they are added into the row accumulator.
+constexpr int kFlush = 64;
+
+template <int SOFT, bool MASSES, int NC, class Acc>
+__device__ __forceinline__ void consume_split(const float4 *stage, int fill, int sub, int kk,
+                                              float px, float py, float pz, const PairArgs &a,
+                                              Acc &acc) {
+    for (int base = sub; base < fill; base += kk * kFlush) {
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        const int end = min(fill, base + kk * kFlush);
+        int j = base;
+        for (; j + 3 * kk < end; j += 4 * kk) {
+            const float4 s0 = stage[j], s1 = stage[j + kk], s2 = stage[j + 2 * kk],
+                         s3 = stage[j + 3 * kk];
+            pair_split<SOFT, MASSES, NC>(s0, px, py, pz, a, ax, ay, az);
+            pair_split<SOFT, MASSES, NC>(s1, px, py, pz, a, ax, ay, az);
+            pair_split<SOFT, MASSES, NC>(s2, px, py, pz, a, ax, ay, az);
+            pair_split<SOFT, MASSES, NC>(s3, px, py, pz, a, ax, ay, az);
+        }
+        for (; j < end; j += kk) pair_split<SOFT, MASSES, NC>(stage[j], px, py, pz, a, ax, ay, az);
+        acc.add(ax, ay, az);
+    }
+}
+
+// Lanes per sink particle group: 32 sink particles per warp pass, or for
+// small slices several lanes share a particle and split its sources.
+__device__ __forceinline__ int group_size(int ns) { return ns > 16 ? 32 : (ns > 8 ? 16 : 8); }
+
+template <int SOFT, bool MASSES, int ACC, int NC>
+__global__ void __launch_bounds__(256)
+pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
+    extern __shared__ float4 smem_f4[];
+    using Acc = typename AccSel<ACC>::T;
+    const int lane = threadIdx.x & 31;
+    float4 *stage = smem_f4 + (threadIdx.x >> 5) * stage_cap;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= a.nleaf) break;
+        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        if (rb >= re) continue;
+        const LeafMeta mt = a.leaf[item];
+        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
+            const int ns = min(32, mt.npart - s0);
+            const int gs = group_size(ns);
+            const int kk = 32 / gs;
+            const int i = lane & (gs - 1), sub = lane / gs;
+            const bool act = i < ns;
+            const float4 p = act ? a.pos4[mt.ipart + s0 + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            Acc acc;
+            int fill = 0;
+            for (int64_t e0 = rb; e0 < re; e0 += 32) {
+                const int ne = (int)min((int64_t)32, re - e0);
+                int sip = 0, snp = 0;
+                float ox = 0.f, oy = 0.f, oz = 0.f;
+                if (lane < ne) {
+                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+                    sip = ms.ipart;
+                    snp = ms.npart;
+                    ox = (float)((ms.cx - mt.cx) * a.cscale);
+                    oy = (float)((ms.cy - mt.cy) * a.cscale);
+                    oz = (float)((ms.cz - mt.cz) * a.cscale);
+                }
+                for (int j = 0; j < ne; ++j) {
+                    const int jnp = __shfl_sync(kFull, snp, j);
+                    const int jip = __shfl_sync(kFull, sip, j);
+                    const float jx = __shfl_sync(kFull, ox, j);
+                    const float jy = __shfl_sync(kFull, oy, j);
+                    const float jz = __shfl_sync(kFull, oz, j);
+                    int q0 = 0;
+                    while (q0 < jnp) {
+                        if (fill == stage_cap) {
+                            __syncwarp();
+                            consume_split<SOFT, MASSES, NC>(stage, fill, sub, kk, p.x, p.y, p.z, a, acc);
+                            __syncwarp();
+                            fill = 0;
+                        }
+                        const int take = min(jnp - q0, stage_cap - fill);
+                        for (int q = lane; q < take; q += 32) {
+                            const float4 v = a.pos4[jip + q0 + q];
+                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
+                        }
+                        fill += take;
+                        q0 += take;
+                    }
+                }
+            }
+            __syncwarp();
+            consume_split<SOFT, MASSES, NC>(stage, fill, sub, kk, p.x, p.y, p.z, a, acc);
+            __syncwarp();
+            acc.reduce_xor(gs);
+            if (act && sub == 0) {
+                const int idx = mt.ipart + s0 + i;
+                a.acc[idx] += acc.vx() * a.out_scale;
+                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
+                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ pair: FP64 ---
+
+// P2P_core_lite (src/gpu_kernel.impl.h:160-257) and P2P_core_1 (:260-362),
+// non-SPI branches, in FP64 with CUDA's erfc / exp / rsqrt.
+template <int SOFT, bool MASSES>
+__device__ __forceinline__ void pair_plain(const double4 s, const double px, const double py,
+                                           const double pz, const PairArgs &a, double &ax,
+                                           double &ay, double &az) {
+    const double dx = s.x - px, dy = s.y - py, dz = s.z - pz;
+    double dr, drs;
+    if (SOFT == SOFT_CLAMP) {
+        const double dr2 = dx * dx + dy * dy + dz * dz;
+        dr = a.soft;
+        if (dr2 > a.soft * a.soft) {
+            const double rdr = rsqrt(dr2);
+            dr = rdr * dr2;
+        }
+        drs = dr * a.hrrs;
+    } else {
+        dr = sqrt(dx * dx + dy * dy + dz * dz + a.soft * a.soft);
+        drs = 0.5 * dr * a.rrs;
+    }
+    if (a.xcut > 0.0 && drs > a.xcut) return;
+    double ir3 = 1.0 / (dr * dr * dr);
+    ir3 *= (erfc(drs) + a.coeff * drs * exp(-drs * drs));
+    if (MASSES) ir3 *= s.w;
+    ax += dx * ir3;
+    ay += dy * ir3;
+    az += dz * ir3;
+}
+
+template <int SOFT, bool MASSES>
+__global__ void __launch_bounds__(256)
+pair_plain_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
+    extern __shared__ double4 smem_d4[];
+    const int lane = threadIdx.x & 31;
+    double4 *stage = smem_d4 + (threadIdx.x >> 5) * stage_cap;
+    const double *X = a.pos, *Y = a.pos + a.npart, *Z = a.pos + 2 * (size_t)a.npart;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= a.nleaf) break;
+        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        if (rb >= re) continue;
+        const LeafMeta mt = a.leaf[item];
+        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
+            const int ns = min(32, mt.npart - s0);
+            const int gs = group_size(ns);
+            const int kk = 32 / gs;
+            const int i = lane & (gs - 1), sub = lane / gs;
+            const bool act = i < ns;
+            const int pi = mt.ipart + s0 + (act ? i : 0);
+            const double px = X[pi], py = Y[pi], pz = Z[pi];
+            double ax = 0.0, ay = 0.0, az = 0.0;
+            int fill = 0;
+            for (int64_t e0 = rb; e0 < re; e0 += 32) {
+                const int ne = (int)min((int64_t)32, re - e0);
+                int sip = 0, snp = 0;
+                if (lane < ne) {
+                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+                    sip = ms.ipart;
+                    snp = ms.npart;
+                }
+                for (int j = 0; j < ne; ++j) {
+                    const int jnp = __shfl_sync(kFull, snp, j);
+                    const int jip = __shfl_sync(kFull, sip, j);
+                    int q0 = 0;
+                    while (q0 < jnp) {
+                        if (fill == stage_cap) {
+                            __syncwarp();
+                            for (int jj = sub; jj < fill; jj += kk)
+                                pair_plain<SOFT, MASSES>(stage[jj], px, py, pz, a, ax, ay, az);
+                            __syncwarp();
+                            fill = 0;
+                        }
+                        const int take = min(jnp - q0, stage_cap - fill);
+                        for (int q = lane; q < take; q += 32) {
+                            const int k = jip + q0 + q;
+                            stage[fill + q] = make_double4(X[k], Y[k], Z[k], a.mass ? a.mass[k] : 1.0);
+                        }
+                        fill += take;
+                        q0 += take;
+                    }
+                }
+            }
+            __syncwarp();
+            for (int jj = sub; jj < fill; jj += kk)
+                pair_plain<SOFT, MASSES>(stage[jj], px, py, pz, a, ax, ay, az);
+            __syncwarp();
+            for (int off = gs; off < 32; off <<= 1) {
+                ax += __shfl_xor_sync(kFull, ax, off);
+                ay += __shfl_xor_sync(kFull, ay, off);
+                az += __shfl_xor_sync(kFull, az, off);
+            }
+            if (act && sub == 0) {
+                const int idx = mt.ipart + s0 + i;
+                const double m = MASSES ? 1.0 : a.mass_eq;
+                a.acc[idx] += ax * m;
+                a.acc[(size_t)a.npart + idx] += ay * m;
+                a.acc[2 * (size_t)a.npart + idx] += az * m;
+            }
+        }
+    }
+}
+
+// --------------------------------------------------------------- probes ---
+
+// FP32 FFMA throughput: 8 independent dependent chains per thread.
+__global__ void __launch_bounds__(256) fma_probe_kernel(float *out, int iters, float m, float b) {
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            x0 = fmaf(x0, m, b); x1 = fmaf(x1, m, b); x2 = fmaf(x2, m, b); x3 = fmaf(x3, m, b);
+            x4 = fmaf(x4, m, b); x5 = fmaf(x5, m, b); x6 = fmaf(x6, m, b); x7 = fmaf(x7, m, b);
+        }
+    }
+    const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace p2p

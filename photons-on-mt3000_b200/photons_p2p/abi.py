@@ -1,0 +1,93 @@
+"""ctypes declarations of the C ABI in include/photons_p2p.h."""
+import ctypes
+
+P2P_OK = 0
+P2P_ERR_ARG = 1
+P2P_ERR_CUDA = 2
+P2P_ERR_STATE = 3
+P2P_ERR_NOMEM = 4
+P2P_ERR_RANGE = 5
+P2P_ERR_CAPACITY = 6
+
+SOFT_CLAMP = 0
+SOFT_PLUMMER = 1
+
+FORM_PLAIN_FP64 = 0
+FORM_SPLIT = 1
+FORM_NAIVE_FP32 = 2
+FORM_KAHAN_FP32 = 3
+
+FORM_NAMES = {
+    FORM_PLAIN_FP64: "plain_fp64",
+    FORM_SPLIT: "split_fp32_fp64",
+    FORM_NAIVE_FP32: "naive_fp32",
+    FORM_KAHAN_FP32: "kahan_fp32",
+}
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("form", ctypes.c_int),
+        ("soft_mode", ctypes.c_int),
+        ("soften", ctypes.c_double),
+        ("split_radius", ctypes.c_double),
+        ("x_cut", ctypes.c_double),
+        ("mass", ctypes.c_double),
+        ("warps_per_block", ctypes.c_int),
+        ("stage_sources", ctypes.c_int),
+        ("blocks_per_sm", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+    ]
+
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "p2p_params_default": (None, [ctypes.POINTER(Params)]),
+    "p2p_status_string": (ctypes.c_char_p, [_i]),
+    "p2p_last_error": (ctypes.c_char_p, []),
+    "p2p_version": (_i, []),
+    "p2p_device_count": (_i, [ctypes.POINTER(_i)]),
+    "p2p_session_create": (_i, [_i, ctypes.POINTER(_vp)]),
+    "p2p_session_destroy": (_i, [_vp]),
+    "p2p_session_set_params": (_i, [_vp, ctypes.POINTER(Params)]),
+    "p2p_session_get_params": (_i, [_vp, ctypes.POINTER(Params)]),
+    "p2p_session_stream": (_vp, [_vp]),
+    "p2p_session_poly_degree": (_i, [_vp]),
+    "p2p_session_poly_error": (_d, [_vp]),
+    "p2p_pass_begin": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "p2p_pass_begin_device": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "p2p_pass_submit": (_i, [_vp, _i64, _vp, _vp]),
+    "p2p_pass_submit_device": (_i, [_vp, _i64, _vp, _vp]),
+    "p2p_pass_end": (_i, [_vp, ctypes.POINTER(_d)]),
+    "p2p_pass_accumulate": (_i, [_vp, _vp]),
+    "p2p_pass_result": (_i, [_vp, _vp]),
+    "p2p_pass_result_device": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "p2p_session_synchronize": (_i, [_vp]),
+    "p2p_pass_pair_count": (_i, [_vp, ctypes.POINTER(_i64)]),
+    "p2p_pass_run_device": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i64, _vp, _vp]),
+    "p2p_kernel_launch_count": (_i64, []),
+    "p2p_session_last_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "p2p_measure_fp32_peak": (_i, [_vp, ctypes.POINTER(_d)]),
+}
+
+
+def declare(lib):
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def header_symbols(header_path):
+    """Function names declared in a C header (for the export test)."""
+    import re
+
+    text = open(header_path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = re.findall(r"\b([a-zA-Z_][a-zA-Z0-9_]*)\s*\([^;{]*\)\s*;", text)
+    return sorted(set(n for n in names if n not in ("if", "while", "for", "sizeof")))

@@ -1,0 +1,157 @@
+"""Session: the P2P force pass through the C ABI of libphotons_p2p.so.
+
+Mirrors the reference's gpu_entry protocol (src/gpu_entry.cu:32-209,
+src/gravity.c:440-449): begin (particles + leaves) -> submit list chunks
+(async) -> end (completion barrier, GPU seconds) -> accumulate (acc += result).
+Errors raise P2PError carrying the library's status code and message; there is
+no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from .abi import (FORM_PLAIN_FP64, P2P_OK, SOFT_CLAMP, Params)
+
+
+class P2PError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"p2p status {status}: {message}")
+        self.status = status
+
+
+def _check(lib, status):
+    if status != P2P_OK:
+        raise P2PError(status, lib.p2p_last_error().decode())
+
+
+def _host(a, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(ctypes.c_void_p)
+
+
+def make_params(form=FORM_PLAIN_FP64, soft_mode=SOFT_CLAMP, soften=1.0, split_radius=1.0,
+                x_cut=2.8125, mass=1.0, warps_per_block=0, stage_sources=0, blocks_per_sm=0):
+    return Params(form, soft_mode, soften, split_radius, x_cut, mass, warps_per_block,
+                  stage_sources, blocks_per_sm, 0)
+
+
+def params_for(cfg, form, mass):
+    """Pass parameters of a workloads.PassConfig."""
+    return make_params(form=form, soft_mode=cfg.soft_mode, soften=cfg.eps,
+                       split_radius=cfg.split_radius, x_cut=cfg.x_cut, mass=mass)
+
+
+class Session:
+    def __init__(self, device=0, params=None):
+        self.lib = _native.core()
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.p2p_session_create(device, ctypes.byref(h)))
+        self.h = h
+        self.npart = 0
+        self._keep = []
+        if params is not None:
+            self.set_params(params)
+
+    def close(self):
+        if self.h:
+            self.lib.p2p_session_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        _check(self.lib, self.lib.p2p_session_set_params(self.h, ctypes.byref(params)))
+
+    @property
+    def stream(self):
+        return self.lib.p2p_session_stream(self.h)
+
+    @property
+    def poly_degree(self):
+        return self.lib.p2p_session_poly_degree(self.h)
+
+    @property
+    def poly_error(self):
+        return self.lib.p2p_session_poly_error(self.h)
+
+    # -- pass protocol on host buffers --------------------------------------
+    def begin(self, pos, leaf_ipart, leaf_npart, masses=None):
+        pos, pp = _host(pos, np.float64)
+        ip, ipp = _host(leaf_ipart, np.int32)
+        npt, npp = _host(leaf_npart, np.int32)
+        mp = None
+        if masses is not None:
+            masses, mp = _host(masses, np.float64)
+        self._keep = [pos, ip, npt, masses]
+        self.npart = pos.shape[-1]
+        _check(self.lib, self.lib.p2p_pass_begin(self.h, self.npart, pp, mp, ip.shape[0], ipp, npp))
+
+    def submit(self, task_t, task_s):
+        tt, tp = _host(task_t, np.int32)
+        ts, sp = _host(task_s, np.int32)
+        self._keep.extend([tt, ts])
+        _check(self.lib, self.lib.p2p_pass_submit(self.h, tt.shape[0], tp, sp))
+
+    def end(self):
+        sec = ctypes.c_double()
+        _check(self.lib, self.lib.p2p_pass_end(self.h, ctypes.byref(sec)))
+        self._keep = []
+        return sec.value
+
+    def accumulate(self, acc):
+        assert acc.dtype == np.float64 and acc.flags.c_contiguous and acc.size == 3 * self.npart
+        _check(self.lib, self.lib.p2p_pass_accumulate(self.h, acc.ctypes.data_as(ctypes.c_void_p)))
+        return acc
+
+    def pair_count(self):
+        v = ctypes.c_int64()
+        _check(self.lib, self.lib.p2p_pass_pair_count(self.h, ctypes.byref(v)))
+        return v.value
+
+    def last_kernel_ms(self):
+        v = ctypes.c_float()
+        _check(self.lib, self.lib.p2p_session_last_kernel_ms(self.h, ctypes.byref(v)))
+        return v.value
+
+    def force_pass(self, pos, leaf_ipart, leaf_npart, task_t, task_s, masses=None, chunk=0):
+        """One complete pass on host arrays; returns (acc (3, npart), gpu_seconds)."""
+        self.begin(pos, leaf_ipart, leaf_npart, masses)
+        n = len(task_t)
+        step = chunk if chunk and chunk > 0 else max(n, 1)
+        for c0 in range(0, n, step):
+            self.submit(task_t[c0:c0 + step], task_s[c0:c0 + step])
+        sec = self.end()
+        acc = np.zeros((3, self.npart), dtype=np.float64)
+        self.accumulate(acc)
+        return acc, sec
+
+    # -- device-resident pass (pointers into HBM, e.g. torch tensors) --------
+    def run_device(self, npart, d_pos, nleaf, d_ip, d_np, ntask, d_t, d_s, d_mass=None):
+        self.npart = npart
+        _check(self.lib, self.lib.p2p_pass_run_device(self.h, npart, d_pos, d_mass, nleaf, d_ip, d_np,
+                                                      ntask, d_t, d_s))
+
+    def result_device(self):
+        p = ctypes.c_void_p()
+        _check(self.lib, self.lib.p2p_pass_result_device(self.h, ctypes.byref(p)))
+        return p.value
+
+    def measure_fp32_peak(self):
+        v = ctypes.c_double()
+        _check(self.lib, self.lib.p2p_measure_fp32_peak(self.h, ctypes.byref(v)))
+        return v.value
+
+
+def kernel_launch_count():
+    return _native.core().p2p_kernel_launch_count()
