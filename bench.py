@@ -1,0 +1,389 @@
+"""Benchmark of the B200 P2P short-range force pass.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                [--workload c2|c1|c2_128] [--form split|plain]
+
+A step is one force pass over the workload's interaction lists. The default
+workload is the 256^3 clustered configuration (60% uniform, 40% in 2,000 NFW
+halos, leaves <= 32, mesh 256, r_s 1.2 cells, cutoff 4.5 r_s, Plummer
+eps 1/40 spacing), generated from a fixed seed (no dataset). Its lists come
+from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
+
+  value    pair-interactions/s of the chosen FP32/FP64-split form, inputs
+           resident in HBM, the whole pass (frame prep, CSR build, pair
+           kernel) replayed as a CUDA graph, device time from CUDA events,
+           L2 flushed between steps (inputs are also larger than L2)
+  e2e      the same metric through the C ABI on pinned host buffers:
+           H2D of positions, leaves and lists, the pass, D2H of the forces
+  roofline FP32 pipe: pairs/s x flops-per-pair (counted from the kernel
+           source, FMA = 2) / the FP32 FFMA peak measured in-process
+
+With --gpus N > 1 (torchrun, one rank per GPU) every rank runs its own
+independent box (replicas, no collective on the data path); the timed
+region is bracketed by barriers and the max over ranks is reported.
+--impl reference times the reference's own P2P arithmetic (P2P_core_lite,
+FP32 SPI, compiled for the host from the reference sources into
+oracle/_ref) on the host cores, over a bounded sample of the same lists.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [REPO, os.path.join(REPO, "photons-on-mt3000_b200")]
+
+from photons_p2p import abi, workloads as W  # noqa: E402
+
+METRIC = "pair-interactions/s"
+
+
+def flops_per_pair(soft_mode, degree, masses=False):
+    """FP32 flops of one pair in pair_split (p2p_kernels.cuh), FMA = 2:
+    dx,dy,dz 3 FADD; u: 3 FFMA (Plummer) or FMUL + 2 FFMA (+FMNMX, clamp);
+    rinv^3 2 FMUL; t = u - u0 1 FADD; Horner `degree` FFMA; f 1 FADD;
+    acc 3 FFMA. MUFU rsqrt and the cutoff select are not flops."""
+    u = 6 if soft_mode == abi.SOFT_PLUMMER else 5
+    return 3 + u + 2 + 1 + 2 * degree + 1 + 6 + (1 if masses else 0)
+
+
+def build_workload(name, rank=0):
+    if name == "c2":
+        cfg, pos = W.c2_config(), W.c2_positions()
+    elif name == "c2_128":
+        cfg = W.scaled(W.c2_config(), name="c2_clustered_128^3", n_side=128, mesh=128,
+                       eps=1.0 / (40 * 128))
+        pos = W.c2_positions(128)
+    elif name == "c1":
+        cfg, pos = W.c1_config(), W.c1_positions()
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    if rank:
+        # replicas: each rank's box is the same configuration, its own draw
+        g = W.rng(1000 + rank)
+        pos = np.mod(pos + g.random((3, 1)), 1.0) * cfg.box + cfg.origin
+    tl = W.prepare(pos, cfg)
+    return cfg, pos.shape[1], tl
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def load_traffic(workload, form_name):
+    """DRAM bytes per launch of the pair kernel from the committed ncu summary
+    for this workload (None when no capture covers it)."""
+    path = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(f"{workload}:{form_name}")
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from photons_p2p.p2p import Session, kernel_launch_count, params_for
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.time()
+    cfg, nlocal, tl = build_workload(args.workload, rank)
+    prep_s = time.time() - t0
+    mass = 1.0 / nlocal
+    P = tl.pair_count()
+    form = abi.FORM_SPLIT if args.form == "split" else abi.FORM_PLAIN_FP64
+
+    d_pos = torch.from_numpy(np.ascontiguousarray(tl.pos)).to(dev)
+    d_ip = torch.from_numpy(tl.leaf_ipart).to(dev)
+    d_np = torch.from_numpy(tl.leaf_npart).to(dev)
+    d_t = torch.from_numpy(tl.task_t).to(dev)
+    d_s = torch.from_numpy(tl.task_s).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+
+    def resident_passes(sess, steps, warmup, sampler=None):
+        stream = torch.cuda.ExternalStream(sess.stream, device=dev)
+        args_dev = (tl.npart, d_pos.data_ptr(), tl.nleaf, d_ip.data_ptr(), d_np.data_ptr(),
+                    tl.ntask, d_t.data_ptr(), d_s.data_ptr())
+        for _ in range(warmup):
+            sess.run_device(*args_dev)
+            sess.end()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        pass_s, kern_ms = [], []
+        l0 = kernel_launch_count()
+        ctx = sampler if sampler is not None else _Null()
+        with ctx:
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1)  # L2 flush, outside the pass events
+                sess.run_device(*args_dev)
+                pass_s.append(sess.end())
+                kern_ms.append(sess.last_kernel_ms())
+        launches = kernel_launch_count() - l0
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return pass_s, kern_ms, launches
+
+    with Session(local) as sess:
+        fp32_peak = sess.measure_fp32_peak()
+        sess.set_params(params_for(cfg, form, mass))
+        degree = sess.poly_degree
+        sampler = ClockSampler(local)
+        pass_s, kern_ms, launches = resident_passes(sess, args.steps, args.warmup, sampler)
+        clocks = sampler.summary()
+        # the plain FP64 form on the same inputs, for the split/plain ratio
+        plain = None
+        if form == abi.FORM_SPLIT and not args.skip_plain:
+            sess.set_params(params_for(cfg, abi.FORM_PLAIN_FP64, mass))
+            p_s, p_k, _ = resident_passes(sess, max(1, min(args.steps, 3)), 1)
+            plain = {"value": P / float(np.mean(p_s)), "kernel_ms": float(np.mean(p_k))}
+            sess.set_params(params_for(cfg, form, mass))
+
+        # e2e through the C ABI on pinned host buffers
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        h_pos, h_ip, h_np, h_t, h_s = (pin(tl.pos), pin(tl.leaf_ipart), pin(tl.leaf_npart),
+                                       pin(tl.task_t), pin(tl.task_s))
+        h_out = torch.zeros((3, tl.npart), dtype=torch.float64).pin_memory()
+        lib = sess.lib
+        import ctypes
+
+        def e2e_pass():
+            ok = lib.p2p_pass_begin(sess.h, tl.npart, h_pos.data_ptr(), None, tl.nleaf,
+                                    h_ip.data_ptr(), h_np.data_ptr())
+            ok |= lib.p2p_pass_submit(sess.h, tl.ntask, h_t.data_ptr(), h_s.data_ptr())
+            ok |= lib.p2p_pass_end(sess.h, ctypes.byref(ctypes.c_double()))
+            ok |= lib.p2p_pass_result(sess.h, h_out.data_ptr())
+            if ok:
+                raise RuntimeError(lib.p2p_last_error().decode())
+
+        for _ in range(max(1, args.warmup)):
+            e2e_pass()
+        e2e_t = []
+        for _ in range(max(1, min(args.steps, 5))):
+            a = time.perf_counter()
+            e2e_pass()
+            e2e_t.append(time.perf_counter() - a)
+        h2d = tl.pos.nbytes + tl.leaf_ipart.nbytes + tl.leaf_npart.nbytes + tl.task_t.nbytes + tl.task_s.nbytes
+        d2h = 3 * tl.npart * 8
+
+    mean_pass = float(np.mean(pass_s))
+    mean_kernel_ms = float(np.mean(kern_ms))
+    total_s = float(np.sum(pass_s))
+    e2e_mean = float(np.mean(e2e_t))
+    if dist:
+        import torch.distributed as tdist
+
+        t = torch.tensor([total_s, e2e_mean], dtype=torch.float64, device=dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_s, e2e_mean = float(t[0]), float(t[1])
+        pt = torch.tensor([float(P)], dtype=torch.float64, device=dev)
+        tdist.all_reduce(pt, op=tdist.ReduceOp.SUM)
+        P_all = float(pt[0])
+    else:
+        P_all = float(P)
+    value = P_all * args.steps / total_s
+    F = flops_per_pair(cfg.soft_mode, degree) if form != abi.FORM_PLAIN_FP64 else None
+    kernel_pairs_per_s = P / (mean_kernel_ms * 1e-3)
+    roofline = None
+    if F:
+        achieved = kernel_pairs_per_s * F / 1e12
+        traffic = load_traffic(args.workload, abi.FORM_NAMES[form])
+        roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak, "traffic": traffic,
+                    "flops_per_pair": F, "peak_source": "FFMA chain microbenchmark in-process (measured)"}
+    out = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 leaf offsets + f64 accumulation)" if form == abi.FORM_SPLIT else "f64",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": cfg.name, "form": abi.FORM_NAMES[form], "n_local": nlocal,
+                   "n_with_ghosts": int(tl.npart), "n_leaf": int(tl.nleaf), "n_task": int(tl.ntask),
+                   "pairs_per_pass": int(P), "leaf_cap": cfg.maxleaf, "mesh": cfg.mesh,
+                   "r_s": cfg.split_radius, "x_cut": cfg.x_cut, "eps": cfg.eps, "soft": "plummer"
+                   if cfg.soft_mode == abi.SOFT_PLUMMER else "clamp", "open_angle": cfg.open_angle,
+                   "poly_degree": degree, "parallelism": f"replicas x{world}",
+                   "l2": "256 MB flush between steps; inputs > L2", "host_prep_s": round(prep_s, 1)},
+        "kernel_ms": mean_kernel_ms,
+        "kernel_pairs_per_s": kernel_pairs_per_s,
+        "roofline": roofline,
+        "plain_fp64": plain,
+        "split_over_plain": (value / plain["value"]) if plain else None,
+        "e2e": {"value": P_all / e2e_mean, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    return out, cfg, tl, nlocal
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def cpu_reference_sample(cfg, tl, mass, target_pairs):
+    """The list entries of the first sink leaves (leaf-id order) whose rows
+    add up to about target_pairs pair interactions."""
+    npart = tl.leaf_npart.astype(np.int64)
+    per_sink = np.bincount(tl.task_t, weights=(npart[tl.task_t] * npart[tl.task_s]).astype(np.float64),
+                           minlength=tl.nleaf)
+    cum = np.cumsum(per_sink)
+    last = min(int(np.searchsorted(cum, target_pairs)), tl.nleaf - 1)
+    sel = tl.task_t <= last
+    return tl.task_t[sel], tl.task_s[sel], int(round(cum[last]))
+
+
+def time_cpu(cfg, tl, mass, target_pairs, steps=1):
+    from oracle import oracle as O
+
+    tt, ts, pairs = cpu_reference_sample(cfg, tl, mass, target_pairs)
+    if O.ref_available("libref_pair.so"):
+        kind = "reference"
+        soft = 0 if cfg.soft_mode == abi.SOFT_CLAMP else 1
+
+        def run():
+            O.ref_p2p_lists("sp_spi", soft, cfg.eps, cfg.split_radius, mass, tl.pos, tl.leaf_ipart,
+                            tl.leaf_npart, tt, ts)
+        what = "reference P2P_core_lite/P2P_core_1 FP32 SPI+GPUCUTOFF (src/gpu_kernel.impl.h, host-compiled), OpenMP over sink leaves"
+    else:
+        kind = "port"
+        prm = O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass)
+
+        def run():
+            O.p2p_lists(prm, tl.pos, tl.leaf_ipart, tl.leaf_npart, tt, ts)
+        what = "oracle/p2p_oracle.c FP64 restatement, OpenMP over sink leaves"
+    times = []
+    for _ in range(steps):
+        a = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - a)
+    v = pairs / float(np.mean(times))
+    return {"value": v, "unit": "pairs/s", "cores": O.num_threads(), "kind": kind,
+            "sample": f"{pairs:.3g} pair interactions ({len(tt)} list entries, first sink rows of {cfg.name}); {what}"}, times
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--form", choices=["split", "plain"], default="split")
+    ap.add_argument("--cpu-pairs", type=float, default=2e9)
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("note: fewer than 3 warm-up steps requested", file=sys.stderr)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+
+    if args.impl == "reference":
+        if rank == 0:
+            t0 = time.time()
+            cfg, nlocal, tl = build_workload(args.workload, 0)
+            mass = 1.0 / nlocal
+            if args.warmup:
+                time_cpu(cfg, tl, mass, min(args.cpu_pairs, 2e8))
+            cb, times = time_cpu(cfg, tl, mass, args.cpu_pairs, steps=args.steps)
+            out = {"metric": METRIC, "value": cb["value"], "unit": "pairs/s", "n_gpus": args.gpus,
+                   "steps": args.steps, "warmup": args.warmup,
+                   "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+                   "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                   "data": "synthetic (seeded; no dataset)",
+                   "config": {"workload": cfg.name, "host_prep_s": round(time.time() - t0, 1)},
+                   "impl": "reference", "cpu_baseline": cb,
+                   "e2e": {"value": cb["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}}
+            print(json.dumps(out), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    out, cfg, tl, nlocal = run_ours(args, rank, world, dist)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb, _ = time_cpu(cfg, tl, 1.0 / nlocal, args.cpu_pairs)
+        out["cpu_baseline"] = cb
+    elif rank == 0:
+        out["cpu_baseline"] = None
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

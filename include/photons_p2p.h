@@ -65,9 +65,14 @@ typedef struct {
     double mass;         /* MASSPART: equal particle mass, used when no masses are given */
     int warps_per_block; /* launch shape of the pair kernel; 0 = default */
     int stage_sources;   /* sources staged per warp in shared memory; 0 = default */
-    int blocks_per_sm;   /* persistent grid = blocks_per_sm * SMs; 0 = default */
-    int reserved;
+    int blocks_per_sm;   /* persistent grid = blocks_per_sm * SMs; 0 = as many as fit */
+    int kernel_variant;  /* FP32 forms: P2P_VARIANT_*; ignored by the FP64 form */
 } p2p_params;
+
+/* Lane mappings of the FP32 pair kernel. */
+#define P2P_VARIANT_AUTO 0        /* the faster mapping (source lanes) */
+#define P2P_VARIANT_SINK_LANES 1  /* one lane per sink particle, sources broadcast */
+#define P2P_VARIANT_SOURCE_LANES 2 /* one lane per staged source, sinks broadcast */
 
 typedef struct p2p_session p2p_session;
 

@@ -55,7 +55,6 @@ void hostfree_task(void) {
     free(task_t);
     task_s = task_t = NULL;
 }
-int print_msg(void) { return 0; }
 double get_last_kntime(int proc_rank) { (void)proc_rank; return 0.0; }
 void hostmalloc_out(int n) { (void)n; }
 void hostfree_out(void) {}

@@ -18,7 +18,7 @@ INCLUDE = os.path.join(REPO, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CUDA_SOURCES = ["p2p_core.cu"]
-CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_internal.h"]
+CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_internal.h", "p2p_fit.h"]
 HOST_SOURCES = ["p2p_lists.cpp"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -8,11 +8,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
 #include "photons_p2p.h"
 #include "p2p_internal.h"
+#include "p2p_fit.h"
 #include "p2p_kernels.cuh"
 
 #define P2P_API extern "C" __attribute__((visibility("default")))
@@ -53,95 +56,6 @@ struct DevBuf {
     size_t cap = 0;
 };
 
-// ----------------------------------------------------------- polynomial ---
-// H(u) = (1 - g(x)) / x^3 with x = sqrt(u), g(x) = erfc(x) + (2/sqrt(pi)) x e^{-x^2}.
-// The power series (4/sqrt(pi)) sum (-1)^n u^n / (n! (2n+3)) follows from
-// g'(x) = -(4/sqrt(pi)) x^2 e^{-x^2}; it is used near 0 where 1 - g cancels.
-double h_exact(double u) {
-    const double k = 4.0 / std::sqrt(M_PI);
-    if (u < 0.25) {
-        double term = 1.0, sum = 0.0;
-        for (int n = 0; n < 30; ++n) {
-            sum += term / (2 * n + 3);
-            term *= -u / (n + 1);
-        }
-        return k * sum;
-    }
-    const double x = std::sqrt(u);
-    const double g = std::erfc(x) + (2.0 / std::sqrt(M_PI)) * x * std::exp(-u);
-    return (1.0 - g) / (x * x * x);
-}
-
-struct PolyFit {
-    int degree = 0;
-    int ncoef_kernel = 0;  // template instance (degree + 1 rounded up)
-    double u0 = 0, umax = 0;
-    double max_err = 0;    // max over [0, umax] of sqrt(u) * |P(u) - H(u)|
-    float coef[kMaxCoef] = {0};
-};
-
-// Chebyshev interpolation of H on [0, umax] (nodes cos(pi (j + 1/2) / (D + 1))),
-// converted to monomials in t = u - u0 with u0 = umax / 2. The degree is the
-// smallest whose interpolation error, weighted by x (the pair force scales
-// as x * dH), stays below tol.
-PolyFit fit_h(double umax, double tol) {
-    static const int kDegrees[] = {8, 10, 12, 14, 16, 20};
-    PolyFit best;
-    const double half = 0.5 * umax;
-    for (int D : kDegrees) {
-        const int n = D + 1;
-        std::vector<double> fj(n), cheb(n);
-        for (int j = 0; j < n; ++j) {
-            const double tau = std::cos(M_PI * (j + 0.5) / n);
-            fj[j] = h_exact(half * (1.0 + tau));
-        }
-        for (int k = 0; k < n; ++k) {
-            double s = 0;
-            for (int j = 0; j < n; ++j) s += fj[j] * std::cos(M_PI * k * (j + 0.5) / n);
-            cheb[k] = (k == 0 ? 1.0 : 2.0) * s / n;
-        }
-        // Chebyshev series -> monomials in tau.
-        std::vector<double> mono(n, 0.0), tkm1(n, 0.0), tk(n, 0.0), tkp1(n, 0.0);
-        tkm1[0] = 1.0;  // T0
-        if (n > 1) tk[1] = 1.0;  // T1
-        for (int k = 0; k < n; ++k) {
-            const std::vector<double> &T = (k == 0) ? tkm1 : tk;
-            for (int m = 0; m < n; ++m) mono[m] += cheb[k] * T[m];
-            if (k >= 1) {
-                std::fill(tkp1.begin(), tkp1.end(), 0.0);
-                for (int m = 0; m + 1 < n; ++m) tkp1[m + 1] += 2.0 * tk[m];
-                for (int m = 0; m < n; ++m) tkp1[m] -= tkm1[m];
-                tkm1 = tk;
-                tk = tkp1;
-            }
-        }
-        // tau = t / half
-        std::vector<double> c(n);
-        double sc = 1.0;
-        for (int m = 0; m < n; ++m) {
-            c[m] = mono[m] / sc;
-            sc *= half;
-        }
-        double err = 0;
-        for (int q = 0; q <= 4000; ++q) {
-            const double u = umax * q / 4000.0;
-            const double t = u - half;
-            double h = c[n - 1];
-            for (int m = n - 2; m >= 0; --m) h = h * t + c[m];
-            err = std::max(err, std::sqrt(u) * std::fabs(h - h_exact(u)));
-        }
-        best.degree = D;
-        best.u0 = half;
-        best.umax = umax;
-        best.max_err = err;
-        std::memset(best.coef, 0, sizeof(best.coef));
-        for (int m = 0; m < n; ++m) best.coef[m] = (float)c[m];
-        best.ncoef_kernel = n;
-        if (err <= tol) break;
-    }
-    return best;
-}
-
 }  // namespace
 }  // namespace p2p
 
@@ -153,6 +67,9 @@ struct p2p_session {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_k0 = nullptr, ev_k1 = nullptr;
     bool kernel_timed = false;
+    bool dry_run = false;  // dispatch without launching (fills the occupancy cache)
+    int last_blocks = 0;
+    std::map<std::tuple<const void *, int, size_t>, int> occupancy;
     p2p_params params{};
     PolyFit fit;
     // device buffers
@@ -217,10 +134,16 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 2048]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
+    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SOURCE_LANES)
+        return fail(P2P_ERR_ARG, "unknown kernel_variant %d", p->kernel_variant);
+    if (p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES &&
+        p->warps_per_block > 4)
+        return fail(P2P_ERR_ARG, "the source-lane kernel runs at most 4 warps per block");
     {
         const int w = p->warps_per_block ? p->warps_per_block : 4;
         const int st = p->stage_sources ? p->stage_sources : (p->form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
-        const size_t smem = (size_t)w * st * (p->form == P2P_FORM_PLAIN_FP64 ? 32 : 16);
+        const bool src = p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES;
+        const size_t smem = (size_t)w * (st + (src ? 32 : 0)) * (p->form == P2P_FORM_PLAIN_FP64 ? 32 : 16);
         if (smem > (size_t)227 * 1024)
             return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
     }
@@ -237,29 +160,55 @@ struct Launch {
     size_t smem;
 };
 
-Launch pair_launch_shape(const p2p_session *s) {
-    Launch L;
-    const bool fp64 = s->params.form == P2P_FORM_PLAIN_FP64;
-    L.warps = s->params.warps_per_block ? s->params.warps_per_block : 4;
-    L.stage = s->params.stage_sources ? s->params.stage_sources : (fp64 ? 128 : 256);
-    L.smem = (size_t)L.warps * L.stage * (fp64 ? sizeof(double4) : sizeof(float4));
-    int per_sm = s->params.blocks_per_sm;
+bool source_lanes(const p2p_params &p) {
+    return p.form != P2P_FORM_PLAIN_FP64 && p.kernel_variant != P2P_VARIANT_SINK_LANES;
+}
+
+// Persistent grid: blocks_per_sm (or as many blocks as the kernel's
+// registers and shared memory let reside) on every SM.
+template <class K>
+int pair_launch_shape(p2p_session *s, K kernel, Launch &L) {
+    const p2p_params &p = s->params;
+    const bool fp64 = p.form == P2P_FORM_PLAIN_FP64;
+    const bool src = source_lanes(p);
+    L.warps = p.warps_per_block ? p.warps_per_block : 4;
+    L.stage = p.stage_sources ? p.stage_sources : (fp64 ? 128 : 256);
+    L.smem = (size_t)L.warps * (L.stage + (src ? 32 : 0)) * (fp64 ? sizeof(double4) : sizeof(float4));
+    int per_sm = p.blocks_per_sm;
     if (!per_sm) {
-        // as many resident blocks as shared memory and 32 warps per SM allow
-        per_sm = std::max(1, std::min(32 / L.warps, (int)(200 * 1024 / std::max<size_t>(L.smem, 1))));
+        // occupancy is queried outside any stream capture (see the dry run in
+        // p2p_pass_run_device) and cached per kernel and shape
+        const auto key = std::make_tuple((const void *)kernel, L.warps, L.smem);
+        auto it = s->occupancy.find(key);
+        if (it == s->occupancy.end()) {
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, L.warps * 32, L.smem));
+            s->occupancy[key] = per_sm;
+        } else {
+            per_sm = it->second;
+        }
+        if (per_sm < 1) return fail(P2P_ERR_ARG, "pair kernel does not fit on an SM with this launch shape");
     }
     L.blocks = per_sm * s->sm_count;
-    return L;
+    return P2P_OK;
 }
 
 template <int SOFT, bool MASSES, int ACC>
-int launch_split_nc(p2p_session *s, const PairArgs &a, const Launch &L) {
+int launch_split_nc(p2p_session *s, const PairArgs &a) {
     const int nc = s->fit.ncoef_kernel;
-#define P2P_NC_CASE(NCV)                                                                      \
-    case NCV: {                                                                               \
-        pair_split_kernel<SOFT, MASSES, ACC, NCV><<<L.blocks, L.warps * 32, L.smem, s->stream>>>( \
-            a, L.stage);                                                                      \
-        break;                                                                                \
+    const bool src = source_lanes(s->params);
+    Launch L;
+#define P2P_NC_CASE(NCV)                                                                       \
+    case NCV: {                                                                                \
+        if (src) {                                                                             \
+            auto k = pair_split_src_kernel<SOFT, MASSES, ACC, NCV>;                            \
+            P2P_TRY(pair_launch_shape(s, k, L));                                               \
+            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
+        } else {                                                                               \
+            auto k = pair_split_kernel<SOFT, MASSES, ACC, NCV>;                                \
+            P2P_TRY(pair_launch_shape(s, k, L));                                               \
+            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
+        }                                                                                      \
+        break;                                                                                 \
     }
     switch (nc) {
         P2P_NC_CASE(9)
@@ -272,43 +221,49 @@ int launch_split_nc(p2p_session *s, const PairArgs &a, const Launch &L) {
             return fail(P2P_ERR_STATE, "no kernel for %d coefficients", nc);
     }
 #undef P2P_NC_CASE
+    if (s->dry_run) return P2P_OK;
     CUDA_TRY(cudaGetLastError());
+    s->last_blocks = L.blocks;
     return launch_count(1);
 }
 
 template <int SOFT, bool MASSES>
-int launch_split_acc(p2p_session *s, const PairArgs &a, const Launch &L) {
+int launch_split_acc(p2p_session *s, const PairArgs &a) {
     switch (s->params.form) {
         case P2P_FORM_SPLIT:
-            return launch_split_nc<SOFT, MASSES, ACC_F64>(s, a, L);
+            return launch_split_nc<SOFT, MASSES, ACC_F64>(s, a);
         case P2P_FORM_KAHAN_FP32:
-            return launch_split_nc<SOFT, MASSES, ACC_KAHAN>(s, a, L);
+            return launch_split_nc<SOFT, MASSES, ACC_KAHAN>(s, a);
         case P2P_FORM_NAIVE_FP32:
-            return launch_split_nc<SOFT, MASSES, ACC_F32>(s, a, L);
+            return launch_split_nc<SOFT, MASSES, ACC_F32>(s, a);
         default:
             return fail(P2P_ERR_STATE, "bad form");
     }
 }
 
 template <int SOFT, bool MASSES>
-int launch_plain(p2p_session *s, const PairArgs &a, const Launch &L) {
-    pair_plain_kernel<SOFT, MASSES><<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage);
+int launch_plain(p2p_session *s, const PairArgs &a) {
+    auto k = pair_plain_kernel<SOFT, MASSES>;
+    Launch L;
+    P2P_TRY(pair_launch_shape(s, k, L));
+    if (s->dry_run) return P2P_OK;
+    k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage);
     CUDA_TRY(cudaGetLastError());
+    s->last_blocks = L.blocks;
     return launch_count(1);
 }
 
 int launch_pair(p2p_session *s, const PairArgs &a) {
-    const Launch L = pair_launch_shape(s);
     const bool masses = a.mass != nullptr;
     const int soft = s->params.soft_mode;
     if (s->params.form == P2P_FORM_PLAIN_FP64) {
         if (soft == P2P_SOFT_CLAMP)
-            return masses ? launch_plain<SOFT_CLAMP, true>(s, a, L) : launch_plain<SOFT_CLAMP, false>(s, a, L);
-        return masses ? launch_plain<SOFT_PLUMMER, true>(s, a, L) : launch_plain<SOFT_PLUMMER, false>(s, a, L);
+            return masses ? launch_plain<SOFT_CLAMP, true>(s, a) : launch_plain<SOFT_CLAMP, false>(s, a);
+        return masses ? launch_plain<SOFT_PLUMMER, true>(s, a) : launch_plain<SOFT_PLUMMER, false>(s, a);
     }
     if (soft == P2P_SOFT_CLAMP)
-        return masses ? launch_split_acc<SOFT_CLAMP, true>(s, a, L) : launch_split_acc<SOFT_CLAMP, false>(s, a, L);
-    return masses ? launch_split_acc<SOFT_PLUMMER, true>(s, a, L) : launch_split_acc<SOFT_PLUMMER, false>(s, a, L);
+        return masses ? launch_split_acc<SOFT_CLAMP, true>(s, a) : launch_split_acc<SOFT_CLAMP, false>(s, a);
+    return masses ? launch_split_acc<SOFT_PLUMMER, true>(s, a) : launch_split_acc<SOFT_PLUMMER, false>(s, a);
 }
 
 // Opt every pair-kernel instance into the largest dynamic shared memory a
@@ -323,7 +278,13 @@ cudaError_t allow_smem_split() {
                         (const void *)pair_split_kernel<SOFT, MASSES, ACC, 13>,
                         (const void *)pair_split_kernel<SOFT, MASSES, ACC, 15>,
                         (const void *)pair_split_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 21>};
+                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 21>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 9>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 11>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 13>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 15>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 17>,
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 21>};
     for (const void *k : ks)
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
     return e;
@@ -441,9 +402,14 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
     launch_count(5);
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
-    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k0, s->stream, cudaEventRecordExternal));
+    // Inside a stream capture the kernel's events become external event-record
+    // nodes of the graph; outside it they are ordinary records.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(s->stream, &cap));
+    const unsigned evflags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0u;
+    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k0, s->stream, evflags));
     P2P_TRY(launch_pair(s, a));
-    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k1, s->stream, cudaEventRecordExternal));
+    if (timed) CUDA_TRY(cudaEventRecordWithFlags(s->ev_k1, s->stream, evflags));
     s->kernel_timed = timed;
     return P2P_OK;
 }
@@ -577,8 +543,7 @@ P2P_API int p2p_session_set_params(p2p_session *s, const p2p_params *params) {
     P2P_TRY(validate_params(params));
     s->params = *params;
     if (is_fp32_form(params->form)) {
-        const double xmax = params->x_cut > 0.0 ? params->x_cut : 4.0;
-        s->fit = fit_h(xmax * xmax, 2e-8);
+        s->fit = fit_h(fit_umax(params->x_cut), 2e-8);
     } else {
         s->fit = PolyFit();
     }
@@ -770,6 +735,12 @@ P2P_API int p2p_pass_run_device(p2p_session *s, int npart, const double *d_pos,
         if (s->gexec) {
             cudaGraphExecDestroy(s->gexec);
             s->gexec = nullptr;
+        }
+        {   // resolve launch shapes (occupancy queries) before capturing
+            s->dry_run = true;
+            const int st = launch_pair(s, make_args(s));
+            s->dry_run = false;
+            if (st != P2P_OK) return st;
         }
         cudaGraph_t graph = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));

@@ -280,9 +280,10 @@ struct AccKahan {
             z += __shfl_xor_sync(kFull, z, off);
         }
     }
-    __device__ __forceinline__ double vx() const { return x; }
-    __device__ __forceinline__ double vy() const { return y; }
-    __device__ __forceinline__ double vz() const { return z; }
+    // compensated value: the running sum minus the carried rounding error
+    __device__ __forceinline__ double vx() const { return (double)x - (double)cx; }
+    __device__ __forceinline__ double vy() const { return (double)y - (double)cy; }
+    __device__ __forceinline__ double vz() const { return (double)z - (double)cz; }
 };
 
 struct AccF32 {
@@ -435,6 +436,147 @@ pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
             acc.reduce_xor(gs);
             if (act && sub == 0) {
                 const int idx = mt.ipart + s0 + i;
+                a.acc[idx] += acc.vx() * a.out_scale;
+                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
+                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
+            }
+        }
+    }
+}
+
+// ------------------------------------------- pair: FP32, source lanes ---
+//
+// Second mapping of the same pass: lanes own staged SOURCES (32 per chunk, so
+// every lane is busy whatever the sink leaf size) and loop over the sink
+// particles of the row, read as shared-memory broadcasts. Each lane keeps an
+// FP32 partial force per sink (registers); every kSrcFlushChunks chunks the
+// 32 lanes' partials are folded with a transposing butterfly (31 shuffles per
+// component) so that lane i holds sink i's sum, which it adds to its FP64
+// (or Kahan / FP32) total.
+constexpr int kSinkGroup = 4;        // sinks evaluated per predicated block
+constexpr int kSrcFlushChunks = 32;  // FP32 partial depth per lane, in chunks
+
+template <int K>
+__device__ __forceinline__ void butterfly_step(float (&v)[32], const int lane) {
+    const bool up = lane & K;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const float send = up ? v[j] : v[j + K];
+        const float keep = up ? v[j + K] : v[j];
+        v[j] = keep + __shfl_xor_sync(kFull, send, K);
+    }
+}
+
+// After the call lane L holds in v[0] the sum over all lanes of v[L].
+__device__ __forceinline__ void transpose_reduce(float (&v)[32], const int lane) {
+    butterfly_step<16>(v, lane);
+    butterfly_step<8>(v, lane);
+    butterfly_step<4>(v, lane);
+    butterfly_step<2>(v, lane);
+    butterfly_step<1>(v, lane);
+}
+
+template <int SOFT, bool MASSES, int NC>
+__device__ __forceinline__ void consume_src_lanes(const float4 *stage, int fill,
+                                                  const float4 *sinks, int ns, int lane,
+                                                  const PairArgs &a, float (&ax)[32],
+                                                  float (&ay)[32], float (&az)[32]) {
+    for (int c = 0; c < fill; c += 32) {
+        const float4 src = (c + lane < fill) ? stage[c + lane]
+                                             : make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+#pragma unroll
+        for (int g = 0; g < 32; g += kSinkGroup) {
+            if (g < ns) {
+#pragma unroll
+                for (int q = 0; q < kSinkGroup; ++q) {
+                    const float4 p = sinks[g + q];
+                    pair_split<SOFT, MASSES, NC>(src, p.x, p.y, p.z, a, ax[g + q], ay[g + q],
+                                                 az[g + q]);
+                }
+            }
+        }
+    }
+}
+
+template <int SOFT, bool MASSES, int ACC, int NC>
+__global__ void __launch_bounds__(128, 3)
+pair_split_src_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
+    extern __shared__ float4 smem_f4[];
+    using Acc = typename AccSel<ACC>::T;
+    const int lane = threadIdx.x & 31;
+    float4 *sinks = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 32);
+    float4 *stage = sinks + 32;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= a.nleaf) break;
+        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        if (rb >= re) continue;
+        const LeafMeta mt = a.leaf[item];
+        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
+            const int ns = min(32, mt.npart - s0);
+            // sinks of this slice in their own leaf frame; slots past ns repeat
+            // the first sink so padded evaluations stay finite (never stored)
+            sinks[lane] = a.pos4[mt.ipart + s0 + (lane < ns ? lane : 0)];
+            float ax[32], ay[32], az[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
+            Acc acc;
+            int fill = 0, chunks = 0;
+            auto flush = [&]() {
+                transpose_reduce(ax, lane);
+                transpose_reduce(ay, lane);
+                transpose_reduce(az, lane);
+                acc.add(ax[0], ay[0], az[0]);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
+                chunks = 0;
+            };
+            auto consume = [&]() {
+                __syncwarp();
+                consume_src_lanes<SOFT, MASSES, NC>(stage, fill, sinks, ns, lane, a, ax, ay, az);
+                __syncwarp();
+                chunks += (fill + 31) >> 5;
+                fill = 0;
+                if (chunks >= kSrcFlushChunks) flush();
+            };
+            for (int64_t e0 = rb; e0 < re; e0 += 32) {
+                const int ne = (int)min((int64_t)32, re - e0);
+                int sip = 0, snp = 0;
+                float ox = 0.f, oy = 0.f, oz = 0.f;
+                if (lane < ne) {
+                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+                    sip = ms.ipart;
+                    snp = ms.npart;
+                    ox = (float)((ms.cx - mt.cx) * a.cscale);
+                    oy = (float)((ms.cy - mt.cy) * a.cscale);
+                    oz = (float)((ms.cz - mt.cz) * a.cscale);
+                }
+                for (int j = 0; j < ne; ++j) {
+                    const int jnp = __shfl_sync(kFull, snp, j);
+                    const int jip = __shfl_sync(kFull, sip, j);
+                    const float jx = __shfl_sync(kFull, ox, j);
+                    const float jy = __shfl_sync(kFull, oy, j);
+                    const float jz = __shfl_sync(kFull, oz, j);
+                    int q0 = 0;
+                    while (q0 < jnp) {
+                        if (fill == stage_cap) consume();
+                        const int take = min(jnp - q0, stage_cap - fill);
+                        for (int q = lane; q < take; q += 32) {
+                            const float4 v = a.pos4[jip + q0 + q];
+                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
+                        }
+                        fill += take;
+                        q0 += take;
+                    }
+                }
+            }
+            if (fill) consume();
+            if (chunks) flush();
+            __syncwarp();  // sinks[] is rewritten by the next slice
+            if (lane < ns) {
+                const int idx = mt.ipart + s0 + lane;
                 a.acc[idx] += acc.vx() * a.out_scale;
                 a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
                 a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;

@@ -17,6 +17,10 @@ FORM_SPLIT = 1
 FORM_NAIVE_FP32 = 2
 FORM_KAHAN_FP32 = 3
 
+VARIANT_AUTO = 0
+VARIANT_SINK_LANES = 1
+VARIANT_SOURCE_LANES = 2
+
 FORM_NAMES = {
     FORM_PLAIN_FP64: "plain_fp64",
     FORM_SPLIT: "split_fp32_fp64",
@@ -36,7 +40,7 @@ class Params(ctypes.Structure):
         ("warps_per_block", ctypes.c_int),
         ("stage_sources", ctypes.c_int),
         ("blocks_per_sm", ctypes.c_int),
-        ("reserved", ctypes.c_int),
+        ("kernel_variant", ctypes.c_int),
     ]
 
 

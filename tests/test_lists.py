@@ -1,0 +1,90 @@
+"""The caller-side tree build and walk (libphotons_lists.so) against the
+reference's own src/fmm.c: identical particle order, leaves and lists."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from photons_p2p import lists as L, workloads as W
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+need_walk = pytest.mark.skipif(not O.ref_available("libref_walk.so"),
+                               reason="oracle/_ref (reference walk) not built")
+
+
+def assert_same(tl, r):
+    assert np.array_equal(tl.perm, r["perm"])
+    assert np.array_equal(tl.leaf_ipart, r["leaf_ipart"])
+    assert np.array_equal(tl.leaf_npart, r["leaf_npart"])
+    assert np.array_equal(tl.leaf_active, r["leaf_active"])
+    assert np.array_equal(tl.leaf_center, r["leaf_center"])
+    assert np.array_equal(tl.leaf_width, r["leaf_width"])
+    assert np.array_equal(tl.task_t, r["task_t"])
+    assert np.array_equal(tl.task_s, r["task_s"])
+
+
+def test_golden_dropin12_walk():
+    g = np.load(os.path.join(GOLDEN, "dropin12.npz"))
+    tl = L.build_tree_lists(g["input_pos"], g["input_tag"], int(g["maxleaf"]), float(g["box"]),
+                            float(g["cutoff_radius"]), float(g["open_angle"]))
+    assert_same(tl, g)
+    assert tl.pair_count() == int(g["pairs"])
+
+
+@need_walk
+@pytest.mark.parametrize("case", ["dropin16", "c1", "clustered32_theta0", "maxleaf256_sampled"])
+def test_walk_matches_reference_live(case):
+    if case == "dropin16":
+        cfg = W.ref_dropin_config(16, 32, 32)
+        pos = W.lattice_gaussian(16, 0.2, W.rng(1))
+    elif case == "c1":
+        cfg, pos = W.c1_config(), W.c1_positions()
+    elif case == "clustered32_theta0":
+        cfg = W.scaled(W.c2_config(), n_side=32, mesh=32, eps=1 / (40 * 32))
+        pos = W.c2_positions(32)
+    else:  # > 1e5 particles: the reference samples the split mean
+        cfg = W.ref_dropin_config(48, 96, 256)
+        pos = W.lattice_gaussian(48, 0.3, W.rng(9))
+    allpos, tag = W.with_ghosts(pos, cfg)
+    tl = L.build_tree_lists(allpos, tag, cfg.maxleaf, cfg.box, cfg.cutoff_radius, cfg.open_angle)
+    r = O.RefWalk("libref_walk.so").run(allpos, tag, cfg.maxleaf, cfg.box, cfg.split_radius,
+                                        cfg.cutoff_radius, cfg.eps, 1.0, cfg.open_angle, 1 << 30)
+    assert_same(tl, r)
+
+
+def test_ghosts_cover_shell():
+    g = W.rng(8)
+    pos = g.random((3, 2000))
+    w = 0.1
+    gp, src = L.make_ghosts(pos, 0.0, 1.0, w)
+    assert gp.shape[1] == src.shape[0] > 0
+    assert np.all((gp > -w) & (gp < 1 + w))
+    assert np.all(np.any((gp < 0) | (gp >= 1), axis=0))  # every ghost is an image outside the box
+    shift = gp - pos[:, src]
+    assert np.allclose(shift, np.round(shift), atol=1e-12)  # integer box shifts
+    # brute force count
+    n = 0
+    for s in np.array(np.meshgrid([-1, 0, 1], [-1, 0, 1], [-1, 0, 1])).reshape(3, -1).T:
+        if not s.any():
+            continue
+        q = pos + s[:, None]
+        n += int(np.sum(np.all((q > -w) & (q < 1 + w), axis=0)))
+    assert n == gp.shape[1]
+
+
+def test_lists_partition_and_symmetry():
+    cfg = W.c1_config()
+    tl = W.prepare(W.c1_positions(), cfg)
+    # leaves partition the particles in order
+    assert tl.leaf_ipart[0] == 0
+    assert np.array_equal(tl.leaf_ipart[1:], np.cumsum(tl.leaf_npart)[:-1])
+    assert tl.leaf_npart.sum() == tl.npart and tl.leaf_npart.max() <= cfg.maxleaf
+    # one-sided lists: (A, B) listed => (B, A) listed when B is active
+    pairs = set(zip(tl.task_t.tolist(), tl.task_s.tolist()))
+    for t, s in list(pairs)[:5000]:
+        if tl.leaf_active[s] >= 0:
+            assert (s, t) in pairs
+    # every active leaf lists itself
+    act = np.nonzero(tl.leaf_active >= 0)[0]
+    assert all((int(a), int(a)) in pairs for a in act)

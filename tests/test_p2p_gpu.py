@@ -1,0 +1,255 @@
+"""Parity of the CUDA P2P pass against the CPU oracle (through the C ABI).
+
+Tolerances (per-particle relative force error |a - a_ref| / |a_ref| over local
+particles):
+  plain FP64 form vs the reference-order oracle:   max <= 1e-12
+  split FP32/FP64 form vs the plain FP64 form:     rms <= 1e-5, max <= 1e-3
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from oracle import oracle as O
+from photons_p2p import abi, workloads as W
+from photons_p2p.p2p import P2PError, Session, make_params, params_for
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_MAX = 1e-12
+SPLIT_RMS = 1e-5
+SPLIT_MAX = 1e-3
+
+
+@pytest.fixture(scope="module")
+def dropin32():
+    """32^3 particles with the reference's own pass settings (clamp softening,
+    GPUCUTOFF, open angle 0.4, r_s 1.25 cells)."""
+    cfg = W.ref_dropin_config(32, 64, 32)
+    pos = W.lattice_gaussian(32, 0.2, W.rng(1))
+    tl = W.prepare(pos, cfg)
+    return cfg, tl, 1.0 / pos.shape[1]
+
+
+@pytest.fixture(scope="module")
+def c1():
+    cfg = W.c1_config()
+    pos = W.c1_positions()
+    tl = W.prepare(pos, cfg)
+    return cfg, tl, 1.0 / pos.shape[1], pos
+
+
+def oracle_acc(cfg, tl, mass, chunk=0, masses=None):
+    prm = O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass)
+    acc, pairs = O.p2p_lists(prm, tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s,
+                             masses=masses, chunk=chunk)
+    return acc, pairs
+
+
+def gpu_acc(cfg, tl, mass, form, chunk=0, masses=None, **launch):
+    with Session(0) as s:
+        prm = params_for(cfg, form, mass)
+        for k, v in launch.items():
+            setattr(prm, k, v)
+        s.set_params(prm)
+        acc, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s,
+                              masses=masses, chunk=chunk)
+        return acc, s.pair_count()
+
+
+def test_plain_matches_oracle_dropin32(gpu, dropin32):
+    cfg, tl, m = dropin32
+    ref, pairs = oracle_acc(cfg, tl, m, chunk=40000)
+    got, gpairs = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64, chunk=40000)
+    assert gpairs == pairs == tl.pair_count()
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert mx <= PLAIN_MAX, (rms, mx)
+
+
+def test_plain_matches_oracle_c1_plummer(gpu, c1):
+    cfg, tl, m, _ = c1
+    ref, _ = oracle_acc(cfg, tl, m)
+    got, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64)
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert mx <= PLAIN_MAX, (rms, mx)
+
+
+VARIANTS = [abi.VARIANT_SINK_LANES, abi.VARIANT_SOURCE_LANES]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("which", ["dropin32", "c1"])
+def test_split_vs_plain(gpu, which, variant, request):
+    cfg, tl, m = request.getfixturevalue(which)[:3]
+    plain, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64)
+    split, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, kernel_variant=variant)
+    rms, mx = rel_err(split, plain, tl.tag == 1)
+    assert rms <= SPLIT_RMS and mx <= SPLIT_MAX, (rms, mx)
+
+
+@pytest.mark.parametrize("form", [abi.FORM_KAHAN_FP32, abi.FORM_NAIVE_FP32])
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_fp32_study_forms(gpu, c1, form, variant):
+    """The precision-study forms stay close to FP64 on a unit box (their
+    differences show at large coordinates, see the precision stress test)."""
+    cfg, tl, m = c1[:3]
+    plain, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64)
+    got, _ = gpu_acc(cfg, tl, m, form, kernel_variant=variant)
+    rms, mx = rel_err(got, plain, tl.tag == 1)
+    assert rms <= 1e-4 and mx <= 1e-2, (rms, mx)
+
+
+def test_plain_equals_direct_oracle_c1(gpu, c1):
+    """Complete lists (open angle 0, x_cut = list cutoff) make the pass equal
+    to the FP64 direct minimum-image sum, independent of the tree."""
+    cfg, tl, m, pos = c1
+    got, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64)
+    g = W.rng(77)
+    n = pos.shape[1]
+    sinks = g.choice(n, 2000, replace=False).astype(np.int32)
+    prm = O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, m)
+    ref = O.direct(prm, pos, cfg.box, sinks)
+    slot = np.empty(tl.npart, np.int64)
+    slot[tl.perm] = np.arange(tl.npart)
+    rms, mx = rel_err(got[:, slot[sinks]], ref)
+    assert mx <= 1e-10, (rms, mx)
+
+
+def test_masses_per_particle(gpu, dropin32):
+    cfg, tl, m = dropin32
+    g = W.rng(5)
+    masses = g.uniform(0.5, 1.5, tl.npart) * m
+    ref, _ = oracle_acc(cfg, tl, m, masses=masses)
+    got, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64, masses=masses)
+    assert rel_err(got, ref, tl.tag == 1)[1] <= PLAIN_MAX
+    split, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, masses=masses)
+    rms, mx = rel_err(split, got, tl.tag == 1)
+    assert rms <= SPLIT_RMS and mx <= SPLIT_MAX, (rms, mx)
+
+
+@pytest.mark.parametrize("form", [abi.FORM_PLAIN_FP64, abi.FORM_SPLIT])
+def test_chunked_submits_equal_single(gpu, dropin32, form):
+    cfg, tl, m = dropin32
+    one, _ = gpu_acc(cfg, tl, m, form)
+    many, _ = gpu_acc(cfg, tl, m, form, chunk=7777)
+    rms, mx = rel_err(many, one, tl.tag == 1)
+    assert mx <= (1e-13 if form == abi.FORM_PLAIN_FP64 else 1e-6), (rms, mx)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("warps,stage,bps", [(1, 32, 0), (2, 64, 1), (4, 512, 0)])
+def test_launch_shapes(gpu, dropin32, warps, stage, bps, variant):
+    cfg, tl, m = dropin32
+    ref, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, kernel_variant=abi.VARIANT_SINK_LANES)
+    got, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, warps_per_block=warps, stage_sources=stage,
+                     blocks_per_sm=bps, kernel_variant=variant)
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert mx <= 1e-5, (rms, mx)
+
+
+def test_big_leaves_maxleaf256(gpu):
+    """The reference's default MAXLEAF = 256: sink leaves span several warp
+    slices and source leaves overflow a small staging buffer."""
+    cfg = W.ref_dropin_config(24, 32, 256)
+    pos = W.lattice_gaussian(24, 0.3, W.rng(11))
+    tl = W.prepare(pos, cfg)
+    assert tl.leaf_npart.max() > 64
+    m = 1.0 / pos.shape[1]
+    ref, _ = oracle_acc(cfg, tl, m)
+    got, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64, stage_sources=64)
+    assert rel_err(got, ref, tl.tag == 1)[1] <= PLAIN_MAX
+    for variant in VARIANTS:
+        split, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, stage_sources=64, kernel_variant=variant)
+        rms, mx = rel_err(split, got, tl.tag == 1)
+        assert rms <= SPLIT_RMS and mx <= SPLIT_MAX, (variant, rms, mx)
+
+
+def test_empty_list_and_zero_particles(gpu):
+    with Session(0) as s:
+        s.set_params(make_params())
+        pos = np.random.default_rng(0).random((3, 10))
+        acc, _ = s.force_pass(pos, [0], [10], np.zeros(0, np.int32), np.zeros(0, np.int32))
+        assert np.all(acc == 0)
+        assert s.pair_count() == 0
+        acc, _ = s.force_pass(np.zeros((3, 0)), [], [], np.zeros(0, np.int32), np.zeros(0, np.int32))
+        assert acc.shape == (3, 0)
+
+
+def test_two_body_known_answer(gpu):
+    """Two particles at separation r, one leaf each; compare to the closed
+    form m * g(r/(2 r_s)) / r^2 and to the oracle's pair function."""
+    from math import erfc, exp, pi, sqrt
+
+    rs, eps, m = 0.01, 1e-4, 0.5
+    for r in (0.003, 0.02, 0.0449, 0.0451):
+        pos = np.array([[0.1, 0.1 + r], [0.2, 0.2], [0.3, 0.3]])
+        for form in (abi.FORM_PLAIN_FP64, abi.FORM_SPLIT):
+            with Session(0, make_params(form=form, soft_mode=abi.SOFT_PLUMMER, soften=eps,
+                                        split_radius=rs, x_cut=2.25, mass=m)) as s:
+                acc, _ = s.force_pass(pos, [0, 1], [1, 1], np.array([0, 0, 1, 1], np.int32),
+                                      np.array([0, 1, 0, 1], np.int32))
+            R = sqrt(r * r + eps * eps)
+            x = R / (2 * rs)
+            want = 0.0 if x > 2.25 else m * r * (erfc(x) + 2 / sqrt(pi) * x * exp(-x * x)) / R ** 3
+            tol = 1e-13 if form == abi.FORM_PLAIN_FP64 else 2e-6
+            if want == 0.0:
+                assert acc[0, 0] == 0.0 and acc[0, 1] == 0.0
+            else:
+                assert abs(acc[0, 0] - want) <= tol * want
+                assert abs(acc[0, 1] + want) <= tol * want
+            assert np.all(acc[1:, :] == 0.0)
+
+
+def test_out_of_range_ids_report_without_fault(gpu):
+    """Bad leaf ids in a list are skipped on the device and reported."""
+    pos = np.random.default_rng(1).random((3, 40))
+    with Session(0, make_params()) as s:
+        s.begin(pos, [0, 20], [20, 20])
+        s.submit(np.array([0, 1, 7, -3], np.int32), np.array([1, 0, 0, 1], np.int32))
+        with pytest.raises(P2PError) as e:
+            s.end()
+        assert e.value.status == abi.P2P_ERR_RANGE
+    with Session(0, make_params()) as s:
+        with pytest.raises(P2PError) as e:
+            s.begin(pos, [0, 30], [20, 20])  # second leaf runs past npart
+        assert e.value.status == abi.P2P_ERR_RANGE
+
+
+def test_protocol_errors(gpu):
+    with Session(0, make_params()) as s:
+        with pytest.raises(P2PError) as e:
+            s.submit(np.zeros(1, np.int32), np.zeros(1, np.int32))
+        assert e.value.status == abi.P2P_ERR_STATE
+        with pytest.raises(P2PError) as e:
+            s.set_params(make_params(soften=0.0))
+        assert e.value.status == abi.P2P_ERR_ARG
+
+
+def test_deterministic_repeat(gpu, dropin32):
+    cfg, tl, m = dropin32
+    a, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT)
+    b, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT)
+    rms, mx = rel_err(a, b, tl.tag == 1)
+    assert mx <= 1e-12, (rms, mx)
+
+
+def test_run_device_graph_matches_host_path(gpu, dropin32):
+    torch = pytest.importorskip("torch")
+    cfg, tl, m = dropin32
+    host, _ = gpu_acc(cfg, tl, m, abi.FORM_SPLIT)
+    dev = torch.device("cuda", 0)
+    d_pos = torch.from_numpy(np.ascontiguousarray(tl.pos)).to(dev)
+    d_ip = torch.from_numpy(tl.leaf_ipart).to(dev)
+    d_np = torch.from_numpy(tl.leaf_npart).to(dev)
+    d_t = torch.from_numpy(tl.task_t).to(dev)
+    d_s = torch.from_numpy(tl.task_s).to(dev)
+    torch.cuda.synchronize()
+    with Session(0, params_for(cfg, abi.FORM_SPLIT, m)) as s:
+        for _ in range(3):  # first call captures the graph, the others replay it
+            s.run_device(tl.npart, d_pos.data_ptr(), tl.nleaf, d_ip.data_ptr(), d_np.data_ptr(),
+                         tl.ntask, d_t.data_ptr(), d_s.data_ptr())
+            s.end()
+            out = np.zeros((3, tl.npart))
+            s.accumulate(out)
+            rms, mx = rel_err(out, host, tl.tag == 1)
+            assert mx <= 1e-12, (rms, mx)
+            assert s.pair_count() == tl.pair_count()
