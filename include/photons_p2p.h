@@ -70,9 +70,10 @@ typedef struct {
 } p2p_params;
 
 /* Lane mappings of the FP32 pair kernel. */
-#define P2P_VARIANT_AUTO 0        /* the faster mapping (source lanes) */
-#define P2P_VARIANT_SINK_LANES 1  /* one lane per sink particle, sources broadcast */
-#define P2P_VARIANT_SOURCE_LANES 2 /* one lane per staged source, sinks broadcast */
+#define P2P_VARIANT_AUTO 0            /* the fastest mapping (P2P_VARIANT_SOURCE_LANES_X2) */
+#define P2P_VARIANT_SINK_LANES 1      /* one lane per sink particle, sources broadcast */
+#define P2P_VARIANT_SOURCE_LANES 2    /* one lane per staged source, sinks broadcast */
+#define P2P_VARIANT_SOURCE_LANES_X2 3 /* source lanes, two sinks per packed f32x2 instruction */
 
 typedef struct p2p_session p2p_session;
 

@@ -134,7 +134,7 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 2048]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
-    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SOURCE_LANES)
+    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SOURCE_LANES_X2)
         return fail(P2P_ERR_ARG, "unknown kernel_variant %d", p->kernel_variant);
     if (p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES &&
         p->warps_per_block > 4)
@@ -162,6 +162,11 @@ struct Launch {
 
 bool source_lanes(const p2p_params &p) {
     return p.form != P2P_FORM_PLAIN_FP64 && p.kernel_variant != P2P_VARIANT_SINK_LANES;
+}
+
+bool packed_lanes(const p2p_params &p) {
+    return p.form != P2P_FORM_PLAIN_FP64 &&
+           (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2);
 }
 
 // Persistent grid: blocks_per_sm (or as many blocks as the kernel's
@@ -196,10 +201,15 @@ template <int SOFT, bool MASSES, int ACC>
 int launch_split_nc(p2p_session *s, const PairArgs &a) {
     const int nc = s->fit.ncoef_kernel;
     const bool src = source_lanes(s->params);
+    const bool x2 = packed_lanes(s->params);
     Launch L;
 #define P2P_NC_CASE(NCV)                                                                       \
     case NCV: {                                                                                \
-        if (src) {                                                                             \
+        if (x2) {                                                                              \
+            auto k = pair_split_src2_kernel<SOFT, MASSES, ACC, NCV>;                           \
+            P2P_TRY(pair_launch_shape(s, k, L));                                               \
+            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
+        } else if (src) {                                                                      \
             auto k = pair_split_src_kernel<SOFT, MASSES, ACC, NCV>;                            \
             P2P_TRY(pair_launch_shape(s, k, L));                                               \
             if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
@@ -284,7 +294,13 @@ cudaError_t allow_smem_split() {
                         (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 13>,
                         (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 15>,
                         (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 21>};
+                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 21>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 9>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 11>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 13>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 15>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 17>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 21>};
     for (const void *k : ks)
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
     return e;
@@ -399,7 +415,15 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
     csr_scatter_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf, row_off,
                                                            (int *)s->fill.p, (int *)s->row_src.p);
     CUDA_TRY(cudaGetLastError());
-    launch_count(5);
+    const int sort_blocks = s->sm_count * 8;
+    csr_sort_rows_warp_kernel<<<grid_for((int64_t)nleaf, 4, sort_blocks), 128, 0, s->stream>>>(
+        row_off, nleaf, (int *)s->row_src.p);
+    csr_sort_rows_block_kernel<<<grid_for((int64_t)nleaf, 1, s->sm_count * 2), kSortBlockThreads, 0,
+                                 s->stream>>>(row_off, nleaf, (int *)s->row_src.p);
+    csr_sort_rows_global_kernel<<<grid_for((int64_t)nleaf, 1, s->sm_count), kSortBlockThreads, 0,
+                                  s->stream>>>(row_off, nleaf, (int *)s->row_src.p);
+    CUDA_TRY(cudaGetLastError());
+    launch_count(8);
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
     // Inside a stream capture the kernel's events become external event-record

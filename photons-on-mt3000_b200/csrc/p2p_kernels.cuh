@@ -157,6 +157,95 @@ __global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__rest
     }
 }
 
+// Rows are sorted by source leaf id after the scatter, so the order in which
+// a row's sources are summed does not depend on the order the atomics
+// placed them in: results are bit-for-bit repeatable.
+//
+// Sorting network: bitonic with "flip" merges, every comparator putting the
+// smaller key at the lower index. Padding a row of length L to the next power
+// of two with +inf keys then never moves a padded key below L, so comparators
+// whose upper index is >= L are simply skipped and no padding is stored.
+template <class Sync>
+__device__ __forceinline__ void flip_bitonic_sort(int *v, int len, int tid, int nthreads,
+                                                  Sync sync) {
+    int P = 1;
+    while (P < len) P <<= 1;
+    for (int size = 2; size <= P; size <<= 1) {
+        const int half = size >> 1;
+        for (int i = tid; i < P / 2; i += nthreads) {
+            const int blk = i / half, off = i % half;
+            const int lo = blk * size + off, hi = blk * size + size - 1 - off;
+            if (hi < len) {
+                const int a = v[lo], b = v[hi];
+                if (a > b) { v[lo] = b; v[hi] = a; }
+            }
+        }
+        sync();
+        for (int stride = half >> 1; stride >= 1; stride >>= 1) {
+            for (int i = tid; i < P / 2; i += nthreads) {
+                const int lo = (i / stride) * 2 * stride + (i % stride), hi = lo + stride;
+                if (hi < len) {
+                    const int a = v[lo], b = v[hi];
+                    if (a > b) { v[lo] = b; v[hi] = a; }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+constexpr int kSortWarpMax = 1024;   // rows up to this length: one warp, shared memory
+constexpr int kSortBlockMax = 8192;  // rows up to this length: one block, shared memory
+constexpr int kSortBlockThreads = 512;
+
+// Rows of length 2..kSortWarpMax, one warp per row (4 warps per block).
+__global__ void __launch_bounds__(128)
+csr_sort_rows_warp_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    __shared__ int buf[4][kSortWarpMax];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *v = buf[w];
+    const int nw = gridDim.x * 4;
+    for (int r = blockIdx.x * 4 + w; r < nleaf; r += nw) {
+        const int64_t b = row_off[r];
+        const int len = (int)(row_off[r + 1] - b);
+        if (len < 2 || len > kSortWarpMax) continue;
+        for (int i = lane; i < len; i += 32) v[i] = row_src[b + i];
+        __syncwarp();
+        flip_bitonic_sort(v, len, lane, 32, []() { __syncwarp(); });
+        for (int i = lane; i < len; i += 32) row_src[b + i] = v[i];
+        __syncwarp();
+    }
+}
+
+// Rows of length kSortWarpMax+1..kSortBlockMax, one block per row.
+__global__ void __launch_bounds__(kSortBlockThreads)
+csr_sort_rows_block_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    __shared__ int v[kSortBlockMax];
+    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
+        const int64_t b = row_off[r];
+        const int len = (int)(row_off[r + 1] - b);
+        if (len <= kSortWarpMax || len > kSortBlockMax) continue;
+        for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = row_src[b + i];
+        __syncthreads();
+        flip_bitonic_sort(v, len, threadIdx.x, blockDim.x, []() { __syncthreads(); });
+        for (int i = threadIdx.x; i < len; i += blockDim.x) row_src[b + i] = v[i];
+        __syncthreads();
+    }
+}
+
+// Longer rows, one block per row, sorted in place in global memory.
+__global__ void __launch_bounds__(kSortBlockThreads)
+csr_sort_rows_global_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
+        const int64_t b = row_off[r];
+        const int64_t len = row_off[r + 1] - b;
+        if (len <= kSortBlockMax) continue;
+        __syncthreads();
+        flip_bitonic_sort(row_src + b, (int)len, threadIdx.x, blockDim.x,
+                          []() { __threadfence_block(); __syncthreads(); });
+    }
+}
+
 // Exclusive scan int32 -> int64 in three kernels. kScanTile elements per block.
 constexpr int kScanThreads = 256;
 constexpr int kScanPer = 8;
@@ -536,6 +625,168 @@ pair_split_src_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
             auto consume = [&]() {
                 __syncwarp();
                 consume_src_lanes<SOFT, MASSES, NC>(stage, fill, sinks, ns, lane, a, ax, ay, az);
+                __syncwarp();
+                chunks += (fill + 31) >> 5;
+                fill = 0;
+                if (chunks >= kSrcFlushChunks) flush();
+            };
+            for (int64_t e0 = rb; e0 < re; e0 += 32) {
+                const int ne = (int)min((int64_t)32, re - e0);
+                int sip = 0, snp = 0;
+                float ox = 0.f, oy = 0.f, oz = 0.f;
+                if (lane < ne) {
+                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+                    sip = ms.ipart;
+                    snp = ms.npart;
+                    ox = (float)((ms.cx - mt.cx) * a.cscale);
+                    oy = (float)((ms.cy - mt.cy) * a.cscale);
+                    oz = (float)((ms.cz - mt.cz) * a.cscale);
+                }
+                for (int j = 0; j < ne; ++j) {
+                    const int jnp = __shfl_sync(kFull, snp, j);
+                    const int jip = __shfl_sync(kFull, sip, j);
+                    const float jx = __shfl_sync(kFull, ox, j);
+                    const float jy = __shfl_sync(kFull, oy, j);
+                    const float jz = __shfl_sync(kFull, oz, j);
+                    int q0 = 0;
+                    while (q0 < jnp) {
+                        if (fill == stage_cap) consume();
+                        const int take = min(jnp - q0, stage_cap - fill);
+                        for (int q = lane; q < take; q += 32) {
+                            const float4 v = a.pos4[jip + q0 + q];
+                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
+                        }
+                        fill += take;
+                        q0 += take;
+                    }
+                }
+            }
+            if (fill) consume();
+            if (chunks) flush();
+            __syncwarp();  // sinks[] is rewritten by the next slice
+            if (lane < ns) {
+                const int idx = mt.ipart + s0 + lane;
+                a.acc[idx] += acc.vx() * a.out_scale;
+                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
+                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
+            }
+        }
+    }
+}
+
+// ------------------------------------ pair: FP32, source lanes, f32x2 ---
+//
+// The source-lane mapping with two sinks per instruction: sm_100's packed
+// FP32 instructions (FFMA2 / FADD2 / FMUL2) evaluate the pair function for
+// sinks i and i+1 against the lane's source at once. Same arithmetic as
+// pair_split element by element; half the FP instructions, twice the
+// independent work per instruction stream.
+
+// Sink pairs in shared memory, coordinates negated so dx = s + (-p).
+struct SinkPair {
+    float4 xy;  // (-x_i, -x_{i+1}, -y_i, -y_{i+1})
+    float2 z;   // (-z_i, -z_{i+1})
+    float2 pad;
+};
+
+constexpr int kPairGroup = 4;  // packed sink pairs (8 sinks) per predicated block
+
+template <int SOFT, bool MASSES, int NC>
+__device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
+                                              const float sw, const SinkPair &p,
+                                              const PairArgs &a, float &ax0, float &ax1,
+                                              float &ay0, float &ay1, float &az0, float &az1) {
+    const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
+    const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
+    const float2 dz = __fadd2_rn(sz, p.z);
+    float2 u;
+    if (SOFT == SOFT_PLUMMER) {
+        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(a.eps2, a.eps2))));
+    } else {
+        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        u.x = fmaxf(u.x, a.eps2);
+        u.y = fmaxf(u.y, a.eps2);
+    }
+    const float2 r = make_float2(rsqrt_approx(u.x), rsqrt_approx(u.y));
+    const float2 r3 = __fmul2_rn(__fmul2_rn(r, r), r);
+    const float2 t = __fadd2_rn(u, make_float2(-a.u0, -a.u0));
+    float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, make_float2(a.coef[k], a.coef[k]));
+    float2 f = __ffma2_rn(h, make_float2(-1.0f, -1.0f), r3);
+    f.x = (u.x <= a.ucut) ? f.x : 0.0f;
+    f.y = (u.y <= a.ucut) ? f.y : 0.0f;
+    if (MASSES) f = __fmul2_rn(f, make_float2(sw, sw));
+    float2 vx = __ffma2_rn(dx, f, make_float2(ax0, ax1));
+    float2 vy = __ffma2_rn(dy, f, make_float2(ay0, ay1));
+    float2 vz = __ffma2_rn(dz, f, make_float2(az0, az1));
+    ax0 = vx.x; ax1 = vx.y;
+    ay0 = vy.x; ay1 = vy.y;
+    az0 = vz.x; az1 = vz.y;
+}
+
+template <int SOFT, bool MASSES, int ACC, int NC>
+__global__ void __launch_bounds__(128, 3)
+pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
+    extern __shared__ float4 smem_f4[];
+    using Acc = typename AccSel<ACC>::T;
+    const int lane = threadIdx.x & 31;
+    float4 *region = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 32);
+    SinkPair *sinks = reinterpret_cast<SinkPair *>(region);  // 16 pairs = 512 B
+    float4 *stage = region + 32;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= a.nleaf) break;
+        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        if (rb >= re) continue;
+        const LeafMeta mt = a.leaf[item];
+        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
+            const int ns = min(32, mt.npart - s0);
+            {
+                // slots past ns repeat the first sink so padded lanes stay finite
+                const float4 q = a.pos4[mt.ipart + s0 + (lane < ns ? lane : 0)];
+                float *xy = reinterpret_cast<float *>(&sinks[lane >> 1].xy);
+                float *z = reinterpret_cast<float *>(&sinks[lane >> 1].z);
+                xy[lane & 1] = -q.x;
+                xy[2 + (lane & 1)] = -q.y;
+                z[lane & 1] = -q.z;
+            }
+            float ax[32], ay[32], az[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
+            Acc acc;
+            int fill = 0, chunks = 0;
+            auto flush = [&]() {
+                transpose_reduce(ax, lane);
+                transpose_reduce(ay, lane);
+                transpose_reduce(az, lane);
+                acc.add(ax[0], ay[0], az[0]);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
+                chunks = 0;
+            };
+            auto consume = [&]() {
+                __syncwarp();
+                for (int c = 0; c < fill; c += 32) {
+                    const float4 src = (c + lane < fill) ? stage[c + lane]
+                                                         : make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+                    const float2 sx = make_float2(src.x, src.x), sy = make_float2(src.y, src.y),
+                                 sz = make_float2(src.z, src.z);
+#pragma unroll
+                    for (int g = 0; g < 16; g += kPairGroup) {
+                        if (2 * g < ns) {
+#pragma unroll
+                            for (int q = 0; q < kPairGroup; ++q) {
+                                const int k = g + q;
+                                pair_split_x2<SOFT, MASSES, NC>(sx, sy, sz, src.w, sinks[k], a,
+                                                                ax[2 * k], ax[2 * k + 1], ay[2 * k],
+                                                                ay[2 * k + 1], az[2 * k], az[2 * k + 1]);
+                            }
+                        }
+                    }
+                }
                 __syncwarp();
                 chunks += (fill + 31) >> 5;
                 fill = 0;

@@ -20,6 +20,7 @@ FORM_KAHAN_FP32 = 3
 VARIANT_AUTO = 0
 VARIANT_SINK_LANES = 1
 VARIANT_SOURCE_LANES = 2
+VARIANT_SOURCE_LANES_X2 = 3
 
 FORM_NAMES = {
     FORM_PLAIN_FP64: "plain_fp64",
