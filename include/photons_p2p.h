@@ -147,6 +147,37 @@ int64_t p2p_kernel_launch_count(void);
  * CUDA events on the session stream (0 if none). Call after p2p_pass_end. */
 int p2p_session_last_kernel_ms(p2p_session *s, float *ms);
 
+/* ---- Allocation-free pass (no counterpart in the reference) ------------
+ * For callers that cannot have a library call cudaMalloc / cudaFree while
+ * they run: codes that reserve nearly all device memory for their own pool
+ * at start-up, processes held to a fixed device-memory quota on a shared GPU,
+ * and pipelines that overlap host work with the GPU (cudaFree synchronises
+ * the device). The pass's scratch is one file-scope __device__ array of
+ * P2P_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits; nothing else is allocated (no cudaMalloc / cudaFree, no
+ * allocating library call, no session).
+ *
+ * Inputs and the output are caller device pointers: d_pos (3*npart doubles,
+ * SoA), the leaf ranges, the (sink, source) list, and d_acc (3*npart doubles,
+ * SoA), which is overwritten with the result. Equal masses (params->mass).
+ * Forms: P2P_FORM_SPLIT (packed source-lane kernel) or P2P_FORM_PLAIN_FP64.
+ * The pass is queued on `stream` (a cudaStream_t, 0 for the default stream)
+ * and the call returns when it has finished there.
+ *
+ * Limit: the scratch needed, about 16*npart (split form only) + 48*nleaf +
+ * 4*ntask bytes plus 256-byte alignment of each piece, must fit in
+ * P2P_NOALLOC_SCRATCH_BYTES; larger passes return P2P_ERR_CAPACITY before
+ * anything is queued. Set-up: the first call on a device resolves the
+ * array's device address with cudaGetSymbolAddress (that device current), so
+ * make the first call on each device before any stream capture. All calls
+ * share the one array: calls whose work overlaps on the GPU (other threads or
+ * streams) race and must be serialised by the caller. Errors are reported by
+ * the status only; p2p_last_error() is not updated by this call. */
+#define P2P_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int p2p_pass_noalloc(const p2p_params *params, int npart, const double *d_pos, int nleaf,
+                     const int *d_leaf_ipart, const int *d_leaf_npart, int64_t ntask,
+                     const int *d_task_t, const int *d_task_s, double *d_acc, void *stream);
+
 /* Measured FP32 FFMA throughput of this GPU (TFLOP/s, FMA = 2 flops) from a
  * dependent-chain microbenchmark run on the session stream. */
 int p2p_measure_fp32_peak(p2p_session *s, double *tflops);

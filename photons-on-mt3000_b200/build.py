@@ -17,7 +17,7 @@ OUT = os.path.join(HERE, "photons_p2p")
 INCLUDE = os.path.join(REPO, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CUDA_SOURCES = ["p2p_core.cu"]
+CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu"]
 CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_internal.h", "p2p_fit.h"]
 HOST_SOURCES = ["p2p_lists.cpp"]
 

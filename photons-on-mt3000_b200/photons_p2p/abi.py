@@ -78,6 +78,7 @@ SIGNATURES = {
     "p2p_kernel_launch_count": (_i64, []),
     "p2p_session_last_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     "p2p_measure_fp32_peak": (_i, [_vp, ctypes.POINTER(_d)]),
+    "p2p_pass_noalloc": (_i, [ctypes.POINTER(Params), _i, _vp, _i, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
 }
 
 
@@ -94,5 +95,6 @@ def header_symbols(header_path):
 
     text = open(header_path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = "\n".join(line for line in text.splitlines() if not line.lstrip().startswith("#"))
     names = re.findall(r"\b([a-zA-Z_][a-zA-Z0-9_]*)\s*\([^;{]*\)\s*;", text)
     return sorted(set(n for n in names if n not in ("if", "while", "for", "sizeof")))
