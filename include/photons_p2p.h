@@ -64,9 +64,13 @@ typedef struct {
                             2.8125, src/gpu_kernel.impl.h:192-196); <= 0: no cutoff */
     double mass;         /* MASSPART: equal particle mass, used when no masses are given */
     int warps_per_block; /* launch shape of the pair kernel; 0 = default */
-    int stage_sources;   /* sources staged per warp in shared memory; 0 = default */
+    int stage_sources;   /* sources staged per warp in shared memory, multiple of 32,
+                            at most 1024; 0 = default */
     int blocks_per_sm;   /* persistent grid = blocks_per_sm * SMs; 0 = as many as fit */
     int kernel_variant;  /* FP32 forms: P2P_VARIANT_*; ignored by the FP64 form */
+    double poly_tol;     /* FP32 forms: bound on x * |dH| of the fitted polynomial
+                            (H: g(x) = 1 - x^3 H(x^2)); the smallest degree meeting it
+                            is used; 0 = default 1e-7 (degree 10 at x_cut 2.25) */
 } p2p_params;
 
 /* Lane mappings of the FP32 pair kernel. */

@@ -17,8 +17,12 @@ OUT = os.path.join(HERE, "photons_p2p")
 INCLUDE = os.path.join(REPO, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu"]
-CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_internal.h", "p2p_fit.h"]
+CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu", "p2p_pair_sink_lanes.cu", "p2p_pair_source_lanes.cu",
+                "p2p_pair_source_lanes_x2.cu", "p2p_pair_source_lanes_x2_kahan.cu",
+                "p2p_pair_source_lanes_x2_f32.cu", "p2p_pair_plain.cu"]
+CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_pass_kernels.cuh", "p2p_pair_kernels.cuh",
+                "p2p_device_common.cuh", "p2p_launch.h", "p2p_internal.h", "p2p_fit.h",
+                "p2p_pair_x2_impl.h"]
 HOST_SOURCES = ["p2p_lists.cpp"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -46,14 +50,23 @@ def build_lists(force=False):
 
 
 def build_cuda(force=False, extra=()):
+    """Each .cu compiles to an object in parallel, then one shared link."""
+    from concurrent.futures import ThreadPoolExecutor
+
     target = os.path.join(OUT, "libphotons_p2p.so")
     srcs = [os.path.join(HERE, "csrc", s) for s in CUDA_SOURCES]
     deps = srcs + [os.path.join(HERE, "csrc", h) for h in CUDA_HEADERS] + [
         os.path.join(INCLUDE, "photons_p2p.h"), __file__]
-    if force or _stale(target, deps):
-        _run([NVCC] + GENCODE + ["-lineinfo", "-O3", "-std=c++17", "--shared",
-                                 "-Xcompiler", "-fPIC,-fvisibility=hidden",
-                                 "-I", INCLUDE, "-o", target] + list(extra) + srcs)
+    if not (force or _stale(target, deps)):
+        return target
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = GENCODE + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+                       "-I", INCLUDE] + list(extra)
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        list(ex.map(lambda so: _run([NVCC] + flags + ["-c", so[0], "-o", so[1]]), zip(srcs, objs)))
+    _run([NVCC] + GENCODE + ["--shared", "-o", target] + objs)
     return target
 
 

@@ -16,7 +16,8 @@
 #include "photons_p2p.h"
 #include "p2p_internal.h"
 #include "p2p_fit.h"
-#include "p2p_kernels.cuh"
+#include "p2p_launch.h"
+#include "p2p_pass_kernels.cuh"
 
 #define P2P_API extern "C" __attribute__((visibility("default")))
 
@@ -128,10 +129,12 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "split_radius must be positive and finite");
     if (!std::isfinite(p->x_cut) || !std::isfinite(p->mass))
         return fail(P2P_ERR_ARG, "x_cut and mass must be finite");
+    if (!(p->poly_tol >= 0.0) || !std::isfinite(p->poly_tol))
+        return fail(P2P_ERR_ARG, "poly_tol must be >= 0");
     if (p->warps_per_block < 0 || p->warps_per_block > 8)
         return fail(P2P_ERR_ARG, "warps_per_block must be in [0, 8]");
-    if (p->stage_sources < 0 || p->stage_sources > 2048 || (p->stage_sources % 32))
-        return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 2048]");
+    if (p->stage_sources < 0 || p->stage_sources > 1024 || (p->stage_sources % 32))
+        return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 1024]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
     if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SOURCE_LANES_X2)
@@ -142,8 +145,8 @@ int validate_params(const p2p_params *p) {
     {
         const int w = p->warps_per_block ? p->warps_per_block : 4;
         const int st = p->stage_sources ? p->stage_sources : (p->form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
-        const bool src = p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES;
-        const size_t smem = (size_t)w * (st + (src ? 32 : 0)) * (p->form == P2P_FORM_PLAIN_FP64 ? 32 : 16);
+        const size_t smem = p->form == P2P_FORM_PLAIN_FP64 ? pair_smem_plain(w, st)
+                            : std::max(pair_smem_x2(w, st), pair_smem_split(w, st, true));
         if (smem > (size_t)227 * 1024)
             return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
     }
@@ -155,11 +158,6 @@ int launch_count(int n) {
     return P2P_OK;
 }
 
-struct Launch {
-    int warps, stage, blocks;
-    size_t smem;
-};
-
 bool source_lanes(const p2p_params &p) {
     return p.form != P2P_FORM_PLAIN_FP64 && p.kernel_variant != P2P_VARIANT_SINK_LANES;
 }
@@ -169,159 +167,47 @@ bool packed_lanes(const p2p_params &p) {
            (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2);
 }
 
-// Persistent grid: blocks_per_sm (or as many blocks as the kernel's
-// registers and shared memory let reside) on every SM.
-template <class K>
-int pair_launch_shape(p2p_session *s, K kernel, Launch &L) {
-    const p2p_params &p = s->params;
-    const bool fp64 = p.form == P2P_FORM_PLAIN_FP64;
-    const bool src = source_lanes(p);
-    L.warps = p.warps_per_block ? p.warps_per_block : 4;
-    L.stage = p.stage_sources ? p.stage_sources : (fp64 ? 128 : 256);
-    L.smem = (size_t)L.warps * (L.stage + (src ? 32 : 0)) * (fp64 ? sizeof(double4) : sizeof(float4));
-    int per_sm = p.blocks_per_sm;
-    if (!per_sm) {
-        // occupancy is queried outside any stream capture (see the dry run in
-        // p2p_pass_run_device) and cached per kernel and shape
-        const auto key = std::make_tuple((const void *)kernel, L.warps, L.smem);
-        auto it = s->occupancy.find(key);
-        if (it == s->occupancy.end()) {
-            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, L.warps * 32, L.smem));
-            s->occupancy[key] = per_sm;
-        } else {
-            per_sm = it->second;
-        }
-        if (per_sm < 1) return fail(P2P_ERR_ARG, "pair kernel does not fit on an SM with this launch shape");
-    }
-    L.blocks = per_sm * s->sm_count;
-    return P2P_OK;
+int default_stage(const p2p_params &p) {
+    return p.stage_sources ? p.stage_sources : (p.form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
 }
 
-template <int SOFT, bool MASSES, int ACC>
-int launch_split_nc(p2p_session *s, const PairArgs &a) {
-    const int nc = s->fit.ncoef_kernel;
-    const bool src = source_lanes(s->params);
-    const bool x2 = packed_lanes(s->params);
-    Launch L;
-#define P2P_NC_CASE(NCV)                                                                       \
-    case NCV: {                                                                                \
-        if (x2) {                                                                              \
-            auto k = pair_split_src2_kernel<SOFT, MASSES, ACC, NCV>;                           \
-            P2P_TRY(pair_launch_shape(s, k, L));                                               \
-            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
-        } else if (src) {                                                                      \
-            auto k = pair_split_src_kernel<SOFT, MASSES, ACC, NCV>;                            \
-            P2P_TRY(pair_launch_shape(s, k, L));                                               \
-            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
-        } else {                                                                               \
-            auto k = pair_split_kernel<SOFT, MASSES, ACC, NCV>;                                \
-            P2P_TRY(pair_launch_shape(s, k, L));                                               \
-            if (!s->dry_run) k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage); \
-        }                                                                                      \
-        break;                                                                                 \
-    }
-    switch (nc) {
-        P2P_NC_CASE(9)
-        P2P_NC_CASE(11)
-        P2P_NC_CASE(13)
-        P2P_NC_CASE(15)
-        P2P_NC_CASE(17)
-        P2P_NC_CASE(21)
-        default:
-            return fail(P2P_ERR_STATE, "no kernel for %d coefficients", nc);
-    }
-#undef P2P_NC_CASE
-    if (s->dry_run) return P2P_OK;
-    CUDA_TRY(cudaGetLastError());
-    s->last_blocks = L.blocks;
-    return launch_count(1);
-}
-
-template <int SOFT, bool MASSES>
-int launch_split_acc(p2p_session *s, const PairArgs &a) {
-    switch (s->params.form) {
-        case P2P_FORM_SPLIT:
-            return launch_split_nc<SOFT, MASSES, ACC_F64>(s, a);
-        case P2P_FORM_KAHAN_FP32:
-            return launch_split_nc<SOFT, MASSES, ACC_KAHAN>(s, a);
-        case P2P_FORM_NAIVE_FP32:
-            return launch_split_nc<SOFT, MASSES, ACC_F32>(s, a);
-        default:
-            return fail(P2P_ERR_STATE, "bad form");
-    }
-}
-
-template <int SOFT, bool MASSES>
-int launch_plain(p2p_session *s, const PairArgs &a) {
-    auto k = pair_plain_kernel<SOFT, MASSES>;
-    Launch L;
-    P2P_TRY(pair_launch_shape(s, k, L));
-    if (s->dry_run) return P2P_OK;
-    k<<<L.blocks, L.warps * 32, L.smem, s->stream>>>(a, L.stage);
-    CUDA_TRY(cudaGetLastError());
-    s->last_blocks = L.blocks;
-    return launch_count(1);
-}
-
+// Dispatch to the lane mapping's launcher (p2p_pair_*.cu).
 int launch_pair(p2p_session *s, const PairArgs &a) {
-    const bool masses = a.mass != nullptr;
-    const int soft = s->params.soft_mode;
-    if (s->params.form == P2P_FORM_PLAIN_FP64) {
-        if (soft == P2P_SOFT_CLAMP)
-            return masses ? launch_plain<SOFT_CLAMP, true>(s, a) : launch_plain<SOFT_CLAMP, false>(s, a);
-        return masses ? launch_plain<SOFT_PLUMMER, true>(s, a) : launch_plain<SOFT_PLUMMER, false>(s, a);
-    }
-    if (soft == P2P_SOFT_CLAMP)
-        return masses ? launch_split_acc<SOFT_CLAMP, true>(s, a) : launch_split_acc<SOFT_CLAMP, false>(s, a);
-    return masses ? launch_split_acc<SOFT_PLUMMER, true>(s, a) : launch_split_acc<SOFT_PLUMMER, false>(s, a);
-}
-
-// Opt every pair-kernel instance into the largest dynamic shared memory a
-// block may use (set once per device, outside any stream capture).
-constexpr int kMaxSmem = 227 * 1024;
-
-template <int SOFT, bool MASSES, int ACC>
-cudaError_t allow_smem_split() {
-    cudaError_t e = cudaSuccess;
-    const void *ks[] = {(const void *)pair_split_kernel<SOFT, MASSES, ACC, 9>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 11>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 13>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 15>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_split_kernel<SOFT, MASSES, ACC, 21>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 9>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 11>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 13>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 15>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_split_src_kernel<SOFT, MASSES, ACC, 21>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 9>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 11>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 13>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 15>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 21>};
-    for (const void *k : ks)
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-    return e;
-}
-
-template <int SOFT, bool MASSES>
-cudaError_t allow_smem_soft() {
-    cudaError_t e = allow_smem_split<SOFT, MASSES, ACC_F64>();
-    if (e == cudaSuccess) e = allow_smem_split<SOFT, MASSES, ACC_KAHAN>();
-    if (e == cudaSuccess) e = allow_smem_split<SOFT, MASSES, ACC_F32>();
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute((const void *)pair_plain_kernel<SOFT, MASSES>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-    return e;
+    const p2p_params &p = s->params;
+    PairLaunch L;
+    L.stream = s->stream;
+    L.sm_count = s->sm_count;
+    L.soft_mode = p.soft_mode == P2P_SOFT_CLAMP ? SOFT_CLAMP : SOFT_PLUMMER;
+    L.masses = a.mass != nullptr;
+    L.acc = p.form == P2P_FORM_KAHAN_FP32 ? ACC_KAHAN : (p.form == P2P_FORM_NAIVE_FP32 ? ACC_F32 : ACC_F64);
+    L.ncoef = s->fit.ncoef_kernel;
+    L.warps = p.warps_per_block ? p.warps_per_block : 4;
+    L.stage = default_stage(p);
+    L.blocks_per_sm = p.blocks_per_sm;
+    L.dry_run = s->dry_run;
+    L.occ = &s->occupancy;
+    PairLaunchResult r;
+    if (p.form == P2P_FORM_PLAIN_FP64)
+        r = launch_pair_plain(L, a);
+    else if (packed_lanes(p))
+        r = launch_pair_source_lanes_x2(L, a);
+    else if (source_lanes(p))
+        r = launch_pair_source_lanes(L, a);
+    else
+        r = launch_pair_sink_lanes(L, a);
+    if (!r.fits) return fail(P2P_ERR_ARG, "pair kernel does not fit on an SM with this launch shape");
+    if (r.cuda != cudaSuccess)
+        return fail(P2P_ERR_CUDA, "pair kernel launch: %s", cudaGetErrorString(r.cuda));
+    if (s->dry_run) return P2P_OK;
+    s->last_blocks = r.blocks;
+    return launch_count(1);
 }
 
 cudaError_t allow_smem_all() {
-    cudaError_t e = allow_smem_soft<SOFT_CLAMP, false>();
-    if (e == cudaSuccess) e = allow_smem_soft<SOFT_CLAMP, true>();
-    if (e == cudaSuccess) e = allow_smem_soft<SOFT_PLUMMER, false>();
-    if (e == cudaSuccess) e = allow_smem_soft<SOFT_PLUMMER, true>();
+    cudaError_t e = allow_smem_sink_lanes();
+    if (e == cudaSuccess) e = allow_smem_source_lanes();
+    if (e == cudaSuccess) e = allow_smem_source_lanes_x2();
+    if (e == cudaSuccess) e = allow_smem_plain();
     return e;
 }
 
@@ -377,7 +263,12 @@ PairArgs make_args(p2p_session *s) {
     a.eps2 = (float)((c * p.soften) * (c * p.soften));
     a.u0 = (float)s->fit.u0;
     a.ucut = (float)s->fit.umax;
-    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = s->fit.coef[k];
+    a.ucut_lo = (float)(s->fit.umax * (1.0 - kCutBand));
+    a.ucut_hi = (float)(s->fit.umax * (1.0 + kCutBand));
+    a.rcut2 = s->fit.umax / (c * c);
+    a.eps2_box = p.soften * p.soften;
+    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = -s->fit.coef[k];
+    a.uin = (float)(s->fit.umax * (1.0 - kInsideMargin));
     a.out_scale = c * c * (s->d_mass ? 1.0 : p.mass);
     a.soft = p.soften;
     a.r_soft = 1.0 / p.soften;
@@ -567,7 +458,7 @@ P2P_API int p2p_session_set_params(p2p_session *s, const p2p_params *params) {
     P2P_TRY(validate_params(params));
     s->params = *params;
     if (is_fp32_form(params->form)) {
-        s->fit = fit_h(fit_umax(params->x_cut), 2e-8);
+        s->fit = fit_h(fit_umax(params->x_cut), params->poly_tol > 0.0 ? params->poly_tol : kDefaultPolyTol);
     } else {
         s->fit = PolyFit();
     }

@@ -11,6 +11,8 @@ namespace p2p {
 struct __align__(16) LeafMeta {
     double cx, cy, cz;
     int ipart, npart;
+    float hx, hy, hz;  // half-extents of the particles' bounding box, scaled by c (FP32 forms)
+    float pad;
 };
 
 // Status bits the device sets instead of faulting on bad input.
@@ -20,6 +22,20 @@ enum : int {
 };
 
 constexpr int kMaxCoef = 21;  // polynomial degree <= 20
+
+// Relative half-width of the cutoff band around x_cut^2 inside which FP32
+// rounding of u cannot decide a pair (coordinate rounding bounds the FP32
+// error of u at about 2.4e-6 relative; the band keeps a 4x margin).
+constexpr double kCutBand = 1.0e-5;
+// Entries whose bound on u is below x_cut^2 (1 - kInsideMargin) cannot hold a
+// band pair; the margin covers the FP32 rounding of the bound itself.
+constexpr double kInsideMargin = 5.0e-5;
+// Default bound on x |dH| of the fitted polynomial.
+constexpr double kDefaultPolyTol = 1.0e-7;
+
+// Template selectors of the pair kernels.
+enum { ACC_F64 = 0, ACC_KAHAN = 1, ACC_F32 = 2 };  // accumulation of the FP32 partials
+enum { SOFT_CLAMP = 0, SOFT_PLUMMER = 1 };         // softening
 
 // Arguments of the pair kernels, passed by value (constant bank).
 struct PairArgs {
@@ -37,9 +53,15 @@ struct PairArgs {
     float u0;                // polynomial expansion point
     float ucut;              // x_cut^2 (or the fitted domain end without cutoff)
     float pad0;
+    // Cutoff band: FP32 u in (ucut_lo, ucut_hi] is too close to the cutoff for
+    // FP32 rounding to decide; such pairs are re-decided from FP64 positions
+    // (box units: r^2 (+ eps^2 for Plummer, max(r^2, eps^2) for clamp) <= rcut2).
+    float ucut_lo, ucut_hi;
+    double rcut2, eps2_box;
     double cscale;           // c
     double out_scale;        // c^2 * mass (equal masses) or c^2 (per-particle masses)
-    float coef[kMaxCoef];    // H(u) ~ sum coef[k] (u - u0)^k
+    float coef[kMaxCoef];    // -H(u) ~ sum coef[k] (u - u0)^k (negated, so f = rinv^2 * rinv + poly)
+    float uin;               // entries whose bound on u stays below uin hold no cutoff-band pair
     // FP64 form (reference units)
     double soft, r_soft, hrrs, rrs, coeff, xcut, mass_eq;
 };

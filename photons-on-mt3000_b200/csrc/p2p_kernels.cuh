@@ -24,939 +24,5 @@
 
 #include "p2p_internal.h"
 
-namespace p2p {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ float rsqrt_approx(float x) {
-    float r;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-// ---------------------------------------------------------------- prep ----
-
-// FP32 forms: frame centres and scaled FP32 coordinates. LOCAL = false puts
-// every leaf's frame at the origin (global FP32 coordinates, the naive form).
-template <bool LOCAL>
-__global__ void prep_split_kernel(const double *__restrict__ pos, const double *__restrict__ mass,
-                                  const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
-                                  int npart, int nleaf, double cscale, LeafMeta *__restrict__ meta,
-                                  float4 *__restrict__ pos4, int *__restrict__ status) {
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; l < nleaf; l += nwarps) {
-        const int ip = leaf_ip[l], np = leaf_np[l];
-        const bool ok = ip >= 0 && np >= 0 && (int64_t)ip + np <= npart;
-        if (!ok) {
-            if (lane == 0) {
-                atomicOr(status, ST_LEAF_RANGE);
-                LeafMeta m;
-                m.cx = m.cy = m.cz = 0.0;
-                m.ipart = 0;
-                m.npart = 0;
-                meta[l] = m;
-            }
-            continue;
-        }
-        const double *X = pos, *Y = pos + npart, *Z = pos + 2 * (size_t)npart;
-        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
-        if (LOCAL && np > 0) {
-            double lo0 = 1e300, lo1 = 1e300, lo2 = 1e300, hi0 = -1e300, hi1 = -1e300, hi2 = -1e300;
-            for (int q = lane; q < np; q += 32) {
-                const double x = X[ip + q], y = Y[ip + q], z = Z[ip + q];
-                lo0 = fmin(lo0, x); hi0 = fmax(hi0, x);
-                lo1 = fmin(lo1, y); hi1 = fmax(hi1, y);
-                lo2 = fmin(lo2, z); hi2 = fmax(hi2, z);
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                lo0 = fmin(lo0, __shfl_xor_sync(kFull, lo0, off));
-                lo1 = fmin(lo1, __shfl_xor_sync(kFull, lo1, off));
-                lo2 = fmin(lo2, __shfl_xor_sync(kFull, lo2, off));
-                hi0 = fmax(hi0, __shfl_xor_sync(kFull, hi0, off));
-                hi1 = fmax(hi1, __shfl_xor_sync(kFull, hi1, off));
-                hi2 = fmax(hi2, __shfl_xor_sync(kFull, hi2, off));
-            }
-            c0 = 0.5 * (lo0 + hi0);
-            c1 = 0.5 * (lo1 + hi1);
-            c2 = 0.5 * (lo2 + hi2);
-        }
-        if (lane == 0) {
-            LeafMeta m;
-            m.cx = c0;
-            m.cy = c1;
-            m.cz = c2;
-            m.ipart = ip;
-            m.npart = np;
-            meta[l] = m;
-        }
-        for (int q = lane; q < np; q += 32) {
-            const int i = ip + q;
-            pos4[i] = make_float4((float)((X[i] - c0) * cscale), (float)((Y[i] - c1) * cscale),
-                                  (float)((Z[i] - c2) * cscale), mass ? (float)mass[i] : 1.0f);
-        }
-    }
-}
-
-// FP64 form: leaf table only (positions stay FP64 SoA).
-__global__ void prep_plain_kernel(const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
-                                  int npart, int nleaf, LeafMeta *__restrict__ meta,
-                                  int *__restrict__ status) {
-    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaf; l += gridDim.x * blockDim.x) {
-        int ip = leaf_ip[l], np = leaf_np[l];
-        if (!(ip >= 0 && np >= 0 && (int64_t)ip + np <= npart)) {
-            atomicOr(status, ST_LEAF_RANGE);
-            ip = 0;
-            np = 0;
-        }
-        LeafMeta m;
-        m.cx = m.cy = m.cz = 0.0;
-        m.ipart = ip;
-        m.npart = np;
-        meta[l] = m;
-    }
-}
-
-// ----------------------------------------------------------------- CSR ----
-
-__global__ void csr_count_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
-                                 int nleaf, const LeafMeta *__restrict__ meta,
-                                 int *__restrict__ counts, unsigned long long *__restrict__ pairs,
-                                 int *__restrict__ status) {
-    __shared__ unsigned long long block_pairs;
-    if (threadIdx.x == 0) block_pairs = 0;
-    __syncthreads();
-    unsigned long long local = 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-        const int t = tt[e], s = ts[e];
-        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) {
-            atomicOr(status, ST_TASK_RANGE);
-            continue;
-        }
-        atomicAdd(&counts[t], 1);
-        local += (unsigned long long)meta[t].npart * (unsigned long long)meta[s].npart;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(kFull, local, off);
-    if ((threadIdx.x & 31) == 0 && local) atomicAdd(&block_pairs, local);
-    __syncthreads();
-    if (threadIdx.x == 0 && block_pairs) atomicAdd(pairs, block_pairs);
-}
-
-__global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
-                                   int nleaf, const int64_t *__restrict__ row_off,
-                                   int *__restrict__ fill, int *__restrict__ row_src) {
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
-        const int t = tt[e], s = ts[e];
-        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) continue;
-        const int k = atomicAdd(&fill[t], 1);
-        row_src[row_off[t] + k] = s;
-    }
-}
-
-// Rows are sorted by source leaf id after the scatter, so the order in which
-// a row's sources are summed does not depend on the order the atomics
-// placed them in: results are bit-for-bit repeatable.
-//
-// Sorting network: bitonic with "flip" merges, every comparator putting the
-// smaller key at the lower index. Padding a row of length L to the next power
-// of two with +inf keys then never moves a padded key below L, so comparators
-// whose upper index is >= L are simply skipped and no padding is stored.
-template <class Sync>
-__device__ __forceinline__ void flip_bitonic_sort(int *v, int len, int tid, int nthreads,
-                                                  Sync sync) {
-    int P = 1;
-    while (P < len) P <<= 1;
-    for (int size = 2; size <= P; size <<= 1) {
-        const int half = size >> 1;
-        for (int i = tid; i < P / 2; i += nthreads) {
-            const int blk = i / half, off = i % half;
-            const int lo = blk * size + off, hi = blk * size + size - 1 - off;
-            if (hi < len) {
-                const int a = v[lo], b = v[hi];
-                if (a > b) { v[lo] = b; v[hi] = a; }
-            }
-        }
-        sync();
-        for (int stride = half >> 1; stride >= 1; stride >>= 1) {
-            for (int i = tid; i < P / 2; i += nthreads) {
-                const int lo = (i / stride) * 2 * stride + (i % stride), hi = lo + stride;
-                if (hi < len) {
-                    const int a = v[lo], b = v[hi];
-                    if (a > b) { v[lo] = b; v[hi] = a; }
-                }
-            }
-            sync();
-        }
-    }
-}
-
-constexpr int kSortWarpMax = 1024;   // rows up to this length: one warp, shared memory
-constexpr int kSortBlockMax = 8192;  // rows up to this length: one block, shared memory
-constexpr int kSortBlockThreads = 512;
-
-// Rows of length 2..kSortWarpMax, one warp per row (4 warps per block).
-__global__ void __launch_bounds__(128)
-csr_sort_rows_warp_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
-    __shared__ int buf[4][kSortWarpMax];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int *v = buf[w];
-    const int nw = gridDim.x * 4;
-    for (int r = blockIdx.x * 4 + w; r < nleaf; r += nw) {
-        const int64_t b = row_off[r];
-        const int len = (int)(row_off[r + 1] - b);
-        if (len < 2 || len > kSortWarpMax) continue;
-        for (int i = lane; i < len; i += 32) v[i] = row_src[b + i];
-        __syncwarp();
-        flip_bitonic_sort(v, len, lane, 32, []() { __syncwarp(); });
-        for (int i = lane; i < len; i += 32) row_src[b + i] = v[i];
-        __syncwarp();
-    }
-}
-
-// Rows of length kSortWarpMax+1..kSortBlockMax, one block per row.
-__global__ void __launch_bounds__(kSortBlockThreads)
-csr_sort_rows_block_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
-    __shared__ int v[kSortBlockMax];
-    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
-        const int64_t b = row_off[r];
-        const int len = (int)(row_off[r + 1] - b);
-        if (len <= kSortWarpMax || len > kSortBlockMax) continue;
-        for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = row_src[b + i];
-        __syncthreads();
-        flip_bitonic_sort(v, len, threadIdx.x, blockDim.x, []() { __syncthreads(); });
-        for (int i = threadIdx.x; i < len; i += blockDim.x) row_src[b + i] = v[i];
-        __syncthreads();
-    }
-}
-
-// Longer rows, one block per row, sorted in place in global memory.
-__global__ void __launch_bounds__(kSortBlockThreads)
-csr_sort_rows_global_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
-    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
-        const int64_t b = row_off[r];
-        const int64_t len = row_off[r + 1] - b;
-        if (len <= kSortBlockMax) continue;
-        __syncthreads();
-        flip_bitonic_sort(row_src + b, (int)len, threadIdx.x, blockDim.x,
-                          []() { __threadfence_block(); __syncthreads(); });
-    }
-}
-
-// Exclusive scan int32 -> int64 in three kernels. kScanTile elements per block.
-constexpr int kScanThreads = 256;
-constexpr int kScanPer = 8;
-constexpr int kScanTile = kScanThreads * kScanPer;
-
-__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t *warp_sums,
-                                                        int64_t *total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int64_t x = v;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int64_t y = __shfl_up_sync(kFull, x, off);
-        if (lane >= off) x += y;
-    }
-    if (lane == 31) warp_sums[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int64_t ws = lane < (kScanThreads / 32) ? warp_sums[lane] : 0;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int64_t y = __shfl_up_sync(kFull, ws, off);
-            if (lane >= off) ws += y;
-        }
-        if (lane < (kScanThreads / 32)) warp_sums[lane] = ws;
-    }
-    __syncthreads();
-    const int64_t before = (w > 0 ? warp_sums[w - 1] : 0) + x - v;
-    if (total) *total = warp_sums[kScanThreads / 32 - 1];
-    return before;
-}
-
-__global__ void __launch_bounds__(kScanThreads)
-scan_tiles_kernel(const int *__restrict__ in, int n, int64_t *__restrict__ out,
-                  int64_t *__restrict__ tile_sums) {
-    __shared__ int64_t warp_sums[kScanThreads / 32];
-    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
-    int64_t v[kScanPer];
-    int64_t s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanPer; ++k) {
-        const int64_t i = base + k;
-        v[k] = i < n ? in[i] : 0;
-        s += v[k];
-    }
-    int64_t total;
-    int64_t run = block_exclusive_scan(s, warp_sums, &total);
-#pragma unroll
-    for (int k = 0; k < kScanPer; ++k) {
-        const int64_t i = base + k;
-        if (i < n) out[i] = run;
-        run += v[k];
-    }
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kScanThreads)
-scan_sums_kernel(int64_t *__restrict__ tile_sums, int ntiles, int64_t *__restrict__ grand_total) {
-    __shared__ int64_t warp_sums[kScanThreads / 32];
-    int64_t carry = 0;
-    for (int b0 = 0; b0 < ntiles; b0 += kScanThreads) {
-        const int i = b0 + threadIdx.x;
-        const int64_t v = i < ntiles ? tile_sums[i] : 0;
-        int64_t total;
-        const int64_t ex = block_exclusive_scan(v, warp_sums, &total);
-        if (i < ntiles) tile_sums[i] = carry + ex;
-        carry += total;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *grand_total = carry;
-}
-
-__global__ void scan_add_kernel(int64_t *__restrict__ out, int n,
-                                const int64_t *__restrict__ tile_sums) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] += tile_sums[i / kScanTile];
-}
-
-// ------------------------------------------------------------ pair: FP32 ---
-
-enum { ACC_F64 = 0, ACC_KAHAN = 1, ACC_F32 = 2 };
-enum { SOFT_CLAMP = 0, SOFT_PLUMMER = 1 };
-
-struct AccF64 {
-    double x = 0.0, y = 0.0, z = 0.0;
-    __device__ __forceinline__ void add(float ax, float ay, float az) {
-        x += (double)ax;
-        y += (double)ay;
-        z += (double)az;
-    }
-    __device__ __forceinline__ void reduce_xor(int from) {
-        for (int off = from; off < 32; off <<= 1) {
-            x += __shfl_xor_sync(kFull, x, off);
-            y += __shfl_xor_sync(kFull, y, off);
-            z += __shfl_xor_sync(kFull, z, off);
-        }
-    }
-    __device__ __forceinline__ double vx() const { return x; }
-    __device__ __forceinline__ double vy() const { return y; }
-    __device__ __forceinline__ double vz() const { return z; }
-};
-
-struct AccKahan {
-    float x = 0.f, y = 0.f, z = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
-    __device__ __forceinline__ static void kadd(float &s, float &c, float v) {
-        const float yv = v - c;
-        const float t = s + yv;
-        c = (t - s) - yv;
-        s = t;
-    }
-    __device__ __forceinline__ void add(float ax, float ay, float az) {
-        kadd(x, cx, ax);
-        kadd(y, cy, ay);
-        kadd(z, cz, az);
-    }
-    __device__ __forceinline__ void reduce_xor(int from) {
-        x -= cx; y -= cy; z -= cz;
-        cx = cy = cz = 0.f;
-        for (int off = from; off < 32; off <<= 1) {
-            x += __shfl_xor_sync(kFull, x, off);
-            y += __shfl_xor_sync(kFull, y, off);
-            z += __shfl_xor_sync(kFull, z, off);
-        }
-    }
-    // compensated value: the running sum minus the carried rounding error
-    __device__ __forceinline__ double vx() const { return (double)x - (double)cx; }
-    __device__ __forceinline__ double vy() const { return (double)y - (double)cy; }
-    __device__ __forceinline__ double vz() const { return (double)z - (double)cz; }
-};
-
-struct AccF32 {
-    float x = 0.f, y = 0.f, z = 0.f;
-    __device__ __forceinline__ void add(float ax, float ay, float az) {
-        x += ax;
-        y += ay;
-        z += az;
-    }
-    __device__ __forceinline__ void reduce_xor(int from) {
-        for (int off = from; off < 32; off <<= 1) {
-            x += __shfl_xor_sync(kFull, x, off);
-            y += __shfl_xor_sync(kFull, y, off);
-            z += __shfl_xor_sync(kFull, z, off);
-        }
-    }
-    __device__ __forceinline__ double vx() const { return x; }
-    __device__ __forceinline__ double vy() const { return y; }
-    __device__ __forceinline__ double vz() const { return z; }
-};
-
-template <int ACC> struct AccSel;
-template <> struct AccSel<ACC_F64> { using T = AccF64; };
-template <> struct AccSel<ACC_KAHAN> { using T = AccKahan; };
-template <> struct AccSel<ACC_F32> { using T = AccF32; };
-
-// One pair in scaled units (lengths times c = 1/(2 r_s)). With u = x^2 the
-// squared (softened) separation, the truncated kernel
-//     g(x) / r^3,   g(x) = erfc(x) + (2/sqrt(pi)) x exp(-x^2)
-// is written as g(x) = 1 - x^3 H(x^2), so that in scaled units
-//     f = rinv^3 - H(u),   H(u) = sum coef[k] (u - u0)^k,
-// a polynomial directly in u: one MUFU rsqrt, no exp, no divide.
-template <int SOFT, bool MASSES, int NC>
-__device__ __forceinline__ void pair_split(const float4 s, const float px, const float py,
-                                           const float pz, const PairArgs &a, float &ax, float &ay,
-                                           float &az) {
-    const float dx = s.x - px, dy = s.y - py, dz = s.z - pz;
-    float u;
-    if (SOFT == SOFT_PLUMMER) {
-        u = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, a.eps2)));
-    } else {
-        u = fmaxf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), a.eps2);
-    }
-    const float rinv = rsqrt_approx(u);
-    const float rinv3 = rinv * rinv * rinv;
-    const float t = u - a.u0;
-    float h = a.coef[NC - 1];
-#pragma unroll
-    for (int k = NC - 2; k >= 0; --k) h = fmaf(h, t, a.coef[k]);
-    float f = rinv3 - h;
-    f = (u <= a.ucut) ? f : 0.0f;
-    if (MASSES) f *= s.w;
-    ax = fmaf(dx, f, ax);
-    ay = fmaf(dy, f, ay);
-    az = fmaf(dz, f, az);
-}
-
-// Staged sources are consumed in FP32 partial sums of at most kFlush
-// sources per lane before they are added into the row accumulator.
-constexpr int kFlush = 64;
-
-template <int SOFT, bool MASSES, int NC, class Acc>
-__device__ __forceinline__ void consume_split(const float4 *stage, int fill, int sub, int kk,
-                                              float px, float py, float pz, const PairArgs &a,
-                                              Acc &acc) {
-    for (int base = sub; base < fill; base += kk * kFlush) {
-        float ax = 0.f, ay = 0.f, az = 0.f;
-        const int end = min(fill, base + kk * kFlush);
-        int j = base;
-        for (; j + 3 * kk < end; j += 4 * kk) {
-            const float4 s0 = stage[j], s1 = stage[j + kk], s2 = stage[j + 2 * kk],
-                         s3 = stage[j + 3 * kk];
-            pair_split<SOFT, MASSES, NC>(s0, px, py, pz, a, ax, ay, az);
-            pair_split<SOFT, MASSES, NC>(s1, px, py, pz, a, ax, ay, az);
-            pair_split<SOFT, MASSES, NC>(s2, px, py, pz, a, ax, ay, az);
-            pair_split<SOFT, MASSES, NC>(s3, px, py, pz, a, ax, ay, az);
-        }
-        for (; j < end; j += kk) pair_split<SOFT, MASSES, NC>(stage[j], px, py, pz, a, ax, ay, az);
-        acc.add(ax, ay, az);
-    }
-}
-
-// Lanes per sink particle group: 32 sink particles per warp pass, or for
-// small slices several lanes share a particle and split its sources.
-__device__ __forceinline__ int group_size(int ns) { return ns > 16 ? 32 : (ns > 8 ? 16 : 8); }
-
-template <int SOFT, bool MASSES, int ACC, int NC>
-__global__ void __launch_bounds__(256)
-pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
-    extern __shared__ float4 smem_f4[];
-    using Acc = typename AccSel<ACC>::T;
-    const int lane = threadIdx.x & 31;
-    float4 *stage = smem_f4 + (threadIdx.x >> 5) * stage_cap;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.queue, 1);
-        item = __shfl_sync(kFull, item, 0);
-        if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
-        if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
-        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
-            const int ns = min(32, mt.npart - s0);
-            const int gs = group_size(ns);
-            const int kk = 32 / gs;
-            const int i = lane & (gs - 1), sub = lane / gs;
-            const bool act = i < ns;
-            const float4 p = act ? a.pos4[mt.ipart + s0 + i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            Acc acc;
-            int fill = 0;
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0;
-                float ox = 0.f, oy = 0.f, oz = 0.f;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                    ox = (float)((ms.cx - mt.cx) * a.cscale);
-                    oy = (float)((ms.cy - mt.cy) * a.cscale);
-                    oz = (float)((ms.cz - mt.cz) * a.cscale);
-                }
-                for (int j = 0; j < ne; ++j) {
-                    const int jnp = __shfl_sync(kFull, snp, j);
-                    const int jip = __shfl_sync(kFull, sip, j);
-                    const float jx = __shfl_sync(kFull, ox, j);
-                    const float jy = __shfl_sync(kFull, oy, j);
-                    const float jz = __shfl_sync(kFull, oz, j);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) {
-                            __syncwarp();
-                            consume_split<SOFT, MASSES, NC>(stage, fill, sub, kk, p.x, p.y, p.z, a, acc);
-                            __syncwarp();
-                            fill = 0;
-                        }
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const float4 v = a.pos4[jip + q0 + q];
-                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-            __syncwarp();
-            consume_split<SOFT, MASSES, NC>(stage, fill, sub, kk, p.x, p.y, p.z, a, acc);
-            __syncwarp();
-            acc.reduce_xor(gs);
-            if (act && sub == 0) {
-                const int idx = mt.ipart + s0 + i;
-                a.acc[idx] += acc.vx() * a.out_scale;
-                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
-                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
-            }
-        }
-    }
-}
-
-// ------------------------------------------- pair: FP32, source lanes ---
-//
-// Second mapping of the same pass: lanes own staged SOURCES (32 per chunk, so
-// every lane is busy whatever the sink leaf size) and loop over the sink
-// particles of the row, read as shared-memory broadcasts. Each lane keeps an
-// FP32 partial force per sink (registers); every kSrcFlushChunks chunks the
-// 32 lanes' partials are folded with a transposing butterfly (31 shuffles per
-// component) so that lane i holds sink i's sum, which it adds to its FP64
-// (or Kahan / FP32) total.
-constexpr int kSinkGroup = 4;        // sinks evaluated per predicated block
-constexpr int kSrcFlushChunks = 32;  // FP32 partial depth per lane, in chunks
-
-template <int K>
-__device__ __forceinline__ void butterfly_step(float (&v)[32], const int lane) {
-    const bool up = lane & K;
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
-        const float send = up ? v[j] : v[j + K];
-        const float keep = up ? v[j + K] : v[j];
-        v[j] = keep + __shfl_xor_sync(kFull, send, K);
-    }
-}
-
-// After the call lane L holds in v[0] the sum over all lanes of v[L].
-__device__ __forceinline__ void transpose_reduce(float (&v)[32], const int lane) {
-    butterfly_step<16>(v, lane);
-    butterfly_step<8>(v, lane);
-    butterfly_step<4>(v, lane);
-    butterfly_step<2>(v, lane);
-    butterfly_step<1>(v, lane);
-}
-
-template <int SOFT, bool MASSES, int NC>
-__device__ __forceinline__ void consume_src_lanes(const float4 *stage, int fill,
-                                                  const float4 *sinks, int ns, int lane,
-                                                  const PairArgs &a, float (&ax)[32],
-                                                  float (&ay)[32], float (&az)[32]) {
-    for (int c = 0; c < fill; c += 32) {
-        const float4 src = (c + lane < fill) ? stage[c + lane]
-                                             : make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
-#pragma unroll
-        for (int g = 0; g < 32; g += kSinkGroup) {
-            if (g < ns) {
-#pragma unroll
-                for (int q = 0; q < kSinkGroup; ++q) {
-                    const float4 p = sinks[g + q];
-                    pair_split<SOFT, MASSES, NC>(src, p.x, p.y, p.z, a, ax[g + q], ay[g + q],
-                                                 az[g + q]);
-                }
-            }
-        }
-    }
-}
-
-template <int SOFT, bool MASSES, int ACC, int NC>
-__global__ void __launch_bounds__(128, 3)
-pair_split_src_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
-    extern __shared__ float4 smem_f4[];
-    using Acc = typename AccSel<ACC>::T;
-    const int lane = threadIdx.x & 31;
-    float4 *sinks = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 32);
-    float4 *stage = sinks + 32;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.queue, 1);
-        item = __shfl_sync(kFull, item, 0);
-        if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
-        if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
-        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
-            const int ns = min(32, mt.npart - s0);
-            // sinks of this slice in their own leaf frame; slots past ns repeat
-            // the first sink so padded evaluations stay finite (never stored)
-            sinks[lane] = a.pos4[mt.ipart + s0 + (lane < ns ? lane : 0)];
-            float ax[32], ay[32], az[32];
-#pragma unroll
-            for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
-            Acc acc;
-            int fill = 0, chunks = 0;
-            auto flush = [&]() {
-                transpose_reduce(ax, lane);
-                transpose_reduce(ay, lane);
-                transpose_reduce(az, lane);
-                acc.add(ax[0], ay[0], az[0]);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
-                chunks = 0;
-            };
-            auto consume = [&]() {
-                __syncwarp();
-                consume_src_lanes<SOFT, MASSES, NC>(stage, fill, sinks, ns, lane, a, ax, ay, az);
-                __syncwarp();
-                chunks += (fill + 31) >> 5;
-                fill = 0;
-                if (chunks >= kSrcFlushChunks) flush();
-            };
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0;
-                float ox = 0.f, oy = 0.f, oz = 0.f;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                    ox = (float)((ms.cx - mt.cx) * a.cscale);
-                    oy = (float)((ms.cy - mt.cy) * a.cscale);
-                    oz = (float)((ms.cz - mt.cz) * a.cscale);
-                }
-                for (int j = 0; j < ne; ++j) {
-                    const int jnp = __shfl_sync(kFull, snp, j);
-                    const int jip = __shfl_sync(kFull, sip, j);
-                    const float jx = __shfl_sync(kFull, ox, j);
-                    const float jy = __shfl_sync(kFull, oy, j);
-                    const float jz = __shfl_sync(kFull, oz, j);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) consume();
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const float4 v = a.pos4[jip + q0 + q];
-                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-            if (fill) consume();
-            if (chunks) flush();
-            __syncwarp();  // sinks[] is rewritten by the next slice
-            if (lane < ns) {
-                const int idx = mt.ipart + s0 + lane;
-                a.acc[idx] += acc.vx() * a.out_scale;
-                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
-                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
-            }
-        }
-    }
-}
-
-// ------------------------------------ pair: FP32, source lanes, f32x2 ---
-//
-// The source-lane mapping with two sinks per instruction: sm_100's packed
-// FP32 instructions (FFMA2 / FADD2 / FMUL2) evaluate the pair function for
-// sinks i and i+1 against the lane's source at once. Same arithmetic as
-// pair_split element by element; half the FP instructions, twice the
-// independent work per instruction stream.
-
-// Sink pairs in shared memory, coordinates negated so dx = s + (-p).
-struct SinkPair {
-    float4 xy;  // (-x_i, -x_{i+1}, -y_i, -y_{i+1})
-    float2 z;   // (-z_i, -z_{i+1})
-    float2 pad;
-};
-
-constexpr int kPairGroup = 4;  // packed sink pairs (8 sinks) per predicated block
-
-template <int SOFT, bool MASSES, int NC>
-__device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
-                                              const float sw, const SinkPair &p,
-                                              const PairArgs &a, float &ax0, float &ax1,
-                                              float &ay0, float &ay1, float &az0, float &az1) {
-    const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
-    const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
-    const float2 dz = __fadd2_rn(sz, p.z);
-    float2 u;
-    if (SOFT == SOFT_PLUMMER) {
-        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(a.eps2, a.eps2))));
-    } else {
-        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-        u.x = fmaxf(u.x, a.eps2);
-        u.y = fmaxf(u.y, a.eps2);
-    }
-    const float2 r = make_float2(rsqrt_approx(u.x), rsqrt_approx(u.y));
-    const float2 r3 = __fmul2_rn(__fmul2_rn(r, r), r);
-    const float2 t = __fadd2_rn(u, make_float2(-a.u0, -a.u0));
-    float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);
-#pragma unroll
-    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, make_float2(a.coef[k], a.coef[k]));
-    float2 f = __ffma2_rn(h, make_float2(-1.0f, -1.0f), r3);
-    f.x = (u.x <= a.ucut) ? f.x : 0.0f;
-    f.y = (u.y <= a.ucut) ? f.y : 0.0f;
-    if (MASSES) f = __fmul2_rn(f, make_float2(sw, sw));
-    float2 vx = __ffma2_rn(dx, f, make_float2(ax0, ax1));
-    float2 vy = __ffma2_rn(dy, f, make_float2(ay0, ay1));
-    float2 vz = __ffma2_rn(dz, f, make_float2(az0, az1));
-    ax0 = vx.x; ax1 = vx.y;
-    ay0 = vy.x; ay1 = vy.y;
-    az0 = vz.x; az1 = vz.y;
-}
-
-template <int SOFT, bool MASSES, int ACC, int NC>
-__global__ void __launch_bounds__(128, 3)
-pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
-    extern __shared__ float4 smem_f4[];
-    using Acc = typename AccSel<ACC>::T;
-    const int lane = threadIdx.x & 31;
-    float4 *region = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 32);
-    SinkPair *sinks = reinterpret_cast<SinkPair *>(region);  // 16 pairs = 512 B
-    float4 *stage = region + 32;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.queue, 1);
-        item = __shfl_sync(kFull, item, 0);
-        if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
-        if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
-        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
-            const int ns = min(32, mt.npart - s0);
-            {
-                // slots past ns repeat the first sink so padded lanes stay finite
-                const float4 q = a.pos4[mt.ipart + s0 + (lane < ns ? lane : 0)];
-                float *xy = reinterpret_cast<float *>(&sinks[lane >> 1].xy);
-                float *z = reinterpret_cast<float *>(&sinks[lane >> 1].z);
-                xy[lane & 1] = -q.x;
-                xy[2 + (lane & 1)] = -q.y;
-                z[lane & 1] = -q.z;
-            }
-            float ax[32], ay[32], az[32];
-#pragma unroll
-            for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
-            Acc acc;
-            int fill = 0, chunks = 0;
-            auto flush = [&]() {
-                transpose_reduce(ax, lane);
-                transpose_reduce(ay, lane);
-                transpose_reduce(az, lane);
-                acc.add(ax[0], ay[0], az[0]);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) ax[i] = ay[i] = az[i] = 0.f;
-                chunks = 0;
-            };
-            auto consume = [&]() {
-                __syncwarp();
-                for (int c = 0; c < fill; c += 32) {
-                    const float4 src = (c + lane < fill) ? stage[c + lane]
-                                                         : make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
-                    const float2 sx = make_float2(src.x, src.x), sy = make_float2(src.y, src.y),
-                                 sz = make_float2(src.z, src.z);
-#pragma unroll
-                    for (int g = 0; g < 16; g += kPairGroup) {
-                        if (2 * g < ns) {
-#pragma unroll
-                            for (int q = 0; q < kPairGroup; ++q) {
-                                const int k = g + q;
-                                pair_split_x2<SOFT, MASSES, NC>(sx, sy, sz, src.w, sinks[k], a,
-                                                                ax[2 * k], ax[2 * k + 1], ay[2 * k],
-                                                                ay[2 * k + 1], az[2 * k], az[2 * k + 1]);
-                            }
-                        }
-                    }
-                }
-                __syncwarp();
-                chunks += (fill + 31) >> 5;
-                fill = 0;
-                if (chunks >= kSrcFlushChunks) flush();
-            };
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0;
-                float ox = 0.f, oy = 0.f, oz = 0.f;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                    ox = (float)((ms.cx - mt.cx) * a.cscale);
-                    oy = (float)((ms.cy - mt.cy) * a.cscale);
-                    oz = (float)((ms.cz - mt.cz) * a.cscale);
-                }
-                for (int j = 0; j < ne; ++j) {
-                    const int jnp = __shfl_sync(kFull, snp, j);
-                    const int jip = __shfl_sync(kFull, sip, j);
-                    const float jx = __shfl_sync(kFull, ox, j);
-                    const float jy = __shfl_sync(kFull, oy, j);
-                    const float jz = __shfl_sync(kFull, oz, j);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) consume();
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const float4 v = a.pos4[jip + q0 + q];
-                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-            if (fill) consume();
-            if (chunks) flush();
-            __syncwarp();  // sinks[] is rewritten by the next slice
-            if (lane < ns) {
-                const int idx = mt.ipart + s0 + lane;
-                a.acc[idx] += acc.vx() * a.out_scale;
-                a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
-                a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
-            }
-        }
-    }
-}
-
-// ------------------------------------------------------------ pair: FP64 ---
-
-// P2P_core_lite (src/gpu_kernel.impl.h:160-257) and P2P_core_1 (:260-362),
-// non-SPI branches, in FP64 with CUDA's erfc / exp / rsqrt.
-template <int SOFT, bool MASSES>
-__device__ __forceinline__ void pair_plain(const double4 s, const double px, const double py,
-                                           const double pz, const PairArgs &a, double &ax,
-                                           double &ay, double &az) {
-    const double dx = s.x - px, dy = s.y - py, dz = s.z - pz;
-    double dr, drs;
-    if (SOFT == SOFT_CLAMP) {
-        const double dr2 = dx * dx + dy * dy + dz * dz;
-        dr = a.soft;
-        if (dr2 > a.soft * a.soft) {
-            const double rdr = rsqrt(dr2);
-            dr = rdr * dr2;
-        }
-        drs = dr * a.hrrs;
-    } else {
-        dr = sqrt(dx * dx + dy * dy + dz * dz + a.soft * a.soft);
-        drs = 0.5 * dr * a.rrs;
-    }
-    if (a.xcut > 0.0 && drs > a.xcut) return;
-    double ir3 = 1.0 / (dr * dr * dr);
-    ir3 *= (erfc(drs) + a.coeff * drs * exp(-drs * drs));
-    if (MASSES) ir3 *= s.w;
-    ax += dx * ir3;
-    ay += dy * ir3;
-    az += dz * ir3;
-}
-
-template <int SOFT, bool MASSES>
-__global__ void __launch_bounds__(256)
-pair_plain_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
-    extern __shared__ double4 smem_d4[];
-    const int lane = threadIdx.x & 31;
-    double4 *stage = smem_d4 + (threadIdx.x >> 5) * stage_cap;
-    const double *X = a.pos, *Y = a.pos + a.npart, *Z = a.pos + 2 * (size_t)a.npart;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.queue, 1);
-        item = __shfl_sync(kFull, item, 0);
-        if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
-        if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
-        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
-            const int ns = min(32, mt.npart - s0);
-            const int gs = group_size(ns);
-            const int kk = 32 / gs;
-            const int i = lane & (gs - 1), sub = lane / gs;
-            const bool act = i < ns;
-            const int pi = mt.ipart + s0 + (act ? i : 0);
-            const double px = X[pi], py = Y[pi], pz = Z[pi];
-            double ax = 0.0, ay = 0.0, az = 0.0;
-            int fill = 0;
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                }
-                for (int j = 0; j < ne; ++j) {
-                    const int jnp = __shfl_sync(kFull, snp, j);
-                    const int jip = __shfl_sync(kFull, sip, j);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) {
-                            __syncwarp();
-                            for (int jj = sub; jj < fill; jj += kk)
-                                pair_plain<SOFT, MASSES>(stage[jj], px, py, pz, a, ax, ay, az);
-                            __syncwarp();
-                            fill = 0;
-                        }
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const int k = jip + q0 + q;
-                            stage[fill + q] = make_double4(X[k], Y[k], Z[k], a.mass ? a.mass[k] : 1.0);
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-            __syncwarp();
-            for (int jj = sub; jj < fill; jj += kk)
-                pair_plain<SOFT, MASSES>(stage[jj], px, py, pz, a, ax, ay, az);
-            __syncwarp();
-            for (int off = gs; off < 32; off <<= 1) {
-                ax += __shfl_xor_sync(kFull, ax, off);
-                ay += __shfl_xor_sync(kFull, ay, off);
-                az += __shfl_xor_sync(kFull, az, off);
-            }
-            if (act && sub == 0) {
-                const int idx = mt.ipart + s0 + i;
-                const double m = MASSES ? 1.0 : a.mass_eq;
-                a.acc[idx] += ax * m;
-                a.acc[(size_t)a.npart + idx] += ay * m;
-                a.acc[2 * (size_t)a.npart + idx] += az * m;
-            }
-        }
-    }
-}
-
-// --------------------------------------------------------------- probes ---
-
-// FP32 FFMA throughput: 8 independent dependent chains per thread.
-__global__ void __launch_bounds__(256) fma_probe_kernel(float *out, int iters, float m, float b) {
-    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
-    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
-    for (int i = 0; i < iters; ++i) {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            x0 = fmaf(x0, m, b); x1 = fmaf(x1, m, b); x2 = fmaf(x2, m, b); x3 = fmaf(x3, m, b);
-            x4 = fmaf(x4, m, b); x5 = fmaf(x5, m, b); x6 = fmaf(x6, m, b); x7 = fmaf(x7, m, b);
-        }
-    }
-    const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
-    if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
-}
-
-}  // namespace p2p
+#include "p2p_pass_kernels.cuh"
+#include "p2p_pair_kernels.cuh"

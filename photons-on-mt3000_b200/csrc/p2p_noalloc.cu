@@ -48,9 +48,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[P2P_NOALLOC_SCR
 std::mutex g_setup_mutex;
 unsigned char *g_scratch_addr[kMaxDevices] = {nullptr};
 
-// Last polynomial fit, reused while x_cut stays the same (no allocation).
+// Last polynomial fit, reused while x_cut and the tolerance stay the same
+// (no allocation).
 std::mutex g_fit_mutex;
-double g_fit_xcut = -1.0;
+double g_fit_xcut = -1.0, g_fit_tol = -1.0;
 PolyFit g_fit;
 
 constexpr size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -171,8 +172,9 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     if (L.total > (size_t)P2P_NOALLOC_SCRATCH_BYTES) return P2P_ERR_CAPACITY;
     const int warps = 4;
     const int stage = p.stage_sources ? p.stage_sources : (fp32 ? 256 : 128);
-    if (stage % 32 || stage > 2048) return P2P_ERR_ARG;
-    const size_t smem = (size_t)warps * (stage + (fp32 ? 32 : 0)) * (fp32 ? sizeof(float4) : sizeof(double4));
+    if (stage % 32 || stage > 1024) return P2P_ERR_ARG;
+    const size_t smem = fp32 ? (size_t)warps * (stage + 64 + stage / 4) * sizeof(float4)
+                             : (size_t)warps * stage * sizeof(double4);
     if (smem > (size_t)227 * 1024) return P2P_ERR_ARG;
 
     int dev = 0, sms = 0;
@@ -188,9 +190,11 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     PolyFit fit;
     if (fp32) {
         std::lock_guard<std::mutex> lock(g_fit_mutex);
-        if (g_fit_xcut != p.x_cut) {
-            g_fit = fit_h(fit_umax(p.x_cut), 2e-8);
+        const double tol = p.poly_tol > 0.0 ? p.poly_tol : kDefaultPolyTol;
+        if (g_fit_xcut != p.x_cut || g_fit_tol != tol) {
+            g_fit = fit_h(fit_umax(p.x_cut), tol);
             g_fit_xcut = p.x_cut;
+            g_fit_tol = tol;
         }
         fit = g_fit;
     }
@@ -260,7 +264,12 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     a.eps2 = (float)((c * p.soften) * (c * p.soften));
     a.u0 = (float)fit.u0;
     a.ucut = (float)fit.umax;
-    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = fit.coef[k];
+    a.ucut_lo = (float)(fit.umax * (1.0 - kCutBand));
+    a.ucut_hi = (float)(fit.umax * (1.0 + kCutBand));
+    a.rcut2 = fit.umax / (c * c);
+    a.eps2_box = p.soften * p.soften;
+    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = -fit.coef[k];
+    a.uin = (float)(fit.umax * (1.0 - kInsideMargin));
     a.out_scale = c * c * p.mass;
     a.soft = p.soften;
     a.r_soft = 1.0 / p.soften;

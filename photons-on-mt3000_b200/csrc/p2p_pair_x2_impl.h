@@ -1,0 +1,70 @@
+// Launch helpers of the packed source-lane kernel for one accumulation mode.
+// Each p2p_pair_source_lanes_x2*.cu instantiates one mode so the instances
+// compile in parallel.
+#pragma once
+
+#include "p2p_launch.h"
+#include "p2p_pair_kernels.cuh"
+
+namespace p2p {
+namespace x2_impl {
+
+template <int SOFT, bool MASSES, int ACC>
+PairLaunchResult by_ncoef(const PairLaunch &L, const PairArgs &a) {
+    const size_t smem = pair_smem_x2(L.warps, L.stage);
+    switch (L.ncoef) {
+        case 9: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 9>, smem, a);
+        case 11: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 11>, smem, a);
+        case 13: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 13>, smem, a);
+        case 15: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 15>, smem, a);
+        case 17: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 17>, smem, a);
+        case 21: return launch_persistent(L, pair_split_src2_kernel<SOFT, MASSES, ACC, 21>, smem, a);
+        default: {
+            PairLaunchResult r;
+            r.cuda = cudaErrorInvalidValue;
+            return r;
+        }
+    }
+}
+
+template <int ACC>
+PairLaunchResult launch(const PairLaunch &L, const PairArgs &a) {
+    if (L.soft_mode == SOFT_CLAMP)
+        return L.masses ? by_ncoef<SOFT_CLAMP, true, ACC>(L, a) : by_ncoef<SOFT_CLAMP, false, ACC>(L, a);
+    return L.masses ? by_ncoef<SOFT_PLUMMER, true, ACC>(L, a) : by_ncoef<SOFT_PLUMMER, false, ACC>(L, a);
+}
+
+template <int SOFT, bool MASSES, int ACC>
+cudaError_t allow_one() {
+    const void *ks[] = {(const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 9>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 11>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 13>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 15>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 17>,
+                        (const void *)pair_split_src2_kernel<SOFT, MASSES, ACC, 21>};
+    cudaError_t e = cudaSuccess;
+    for (const void *k : ks)
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return e;
+}
+
+template <int ACC>
+cudaError_t allow() {
+    cudaError_t e = allow_one<SOFT_CLAMP, false, ACC>();
+    if (e == cudaSuccess) e = allow_one<SOFT_CLAMP, true, ACC>();
+    if (e == cudaSuccess) e = allow_one<SOFT_PLUMMER, false, ACC>();
+    if (e == cudaSuccess) e = allow_one<SOFT_PLUMMER, true, ACC>();
+    return e;
+}
+
+}  // namespace x2_impl
+
+// one function pair per accumulation mode (p2p_pair_source_lanes_x2{,_kahan,_f32}.cu)
+PairLaunchResult launch_x2_f64(const PairLaunch &L, const PairArgs &a);
+PairLaunchResult launch_x2_kahan(const PairLaunch &L, const PairArgs &a);
+PairLaunchResult launch_x2_f32(const PairLaunch &L, const PairArgs &a);
+cudaError_t allow_x2_f64();
+cudaError_t allow_x2_kahan();
+cudaError_t allow_x2_f32();
+
+}  // namespace p2p

@@ -1,0 +1,327 @@
+// Pass kernels: frame preparation, CSR build (count, scan, scatter, row
+// sort) and the FP32 throughput probe. Non-template kernels: a translation
+// unit that includes this header defines them.
+#pragma once
+
+#include "p2p_device_common.cuh"
+
+namespace p2p {
+
+// ---------------------------------------------------------------- prep ----
+
+// FP32 forms: frame centres and scaled FP32 coordinates. LOCAL = false puts
+// every leaf's frame at the origin (global FP32 coordinates, the naive form).
+template <bool LOCAL>
+__global__ void prep_split_kernel(const double *__restrict__ pos, const double *__restrict__ mass,
+                                  const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
+                                  int npart, int nleaf, double cscale, LeafMeta *__restrict__ meta,
+                                  float4 *__restrict__ pos4, int *__restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int l = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; l < nleaf; l += nwarps) {
+        const int ip = leaf_ip[l], np = leaf_np[l];
+        const bool ok = ip >= 0 && np >= 0 && (int64_t)ip + np <= npart;
+        if (!ok) {
+            if (lane == 0) {
+                atomicOr(status, ST_LEAF_RANGE);
+                LeafMeta m;
+                m.cx = m.cy = m.cz = 0.0;
+                m.ipart = 0;
+                m.npart = 0;
+                m.hx = m.hy = m.hz = m.pad = 0.f;
+                meta[l] = m;
+            }
+            continue;
+        }
+        const double *X = pos, *Y = pos + npart, *Z = pos + 2 * (size_t)npart;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        float e0 = 0.f, e1 = 0.f, e2 = 0.f;
+        if (LOCAL && np > 0) {
+            double lo0 = 1e300, lo1 = 1e300, lo2 = 1e300, hi0 = -1e300, hi1 = -1e300, hi2 = -1e300;
+            for (int q = lane; q < np; q += 32) {
+                const double x = X[ip + q], y = Y[ip + q], z = Z[ip + q];
+                lo0 = fmin(lo0, x); hi0 = fmax(hi0, x);
+                lo1 = fmin(lo1, y); hi1 = fmax(hi1, y);
+                lo2 = fmin(lo2, z); hi2 = fmax(hi2, z);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                lo0 = fmin(lo0, __shfl_xor_sync(kFull, lo0, off));
+                lo1 = fmin(lo1, __shfl_xor_sync(kFull, lo1, off));
+                lo2 = fmin(lo2, __shfl_xor_sync(kFull, lo2, off));
+                hi0 = fmax(hi0, __shfl_xor_sync(kFull, hi0, off));
+                hi1 = fmax(hi1, __shfl_xor_sync(kFull, hi1, off));
+                hi2 = fmax(hi2, __shfl_xor_sync(kFull, hi2, off));
+            }
+            c0 = 0.5 * (lo0 + hi0);
+            c1 = 0.5 * (lo1 + hi1);
+            c2 = 0.5 * (lo2 + hi2);
+            // half-extents, rounded up: a bound, never an underestimate
+            e0 = __double2float_ru(0.5 * (hi0 - lo0) * cscale * (1.0 + 1e-6));
+            e1 = __double2float_ru(0.5 * (hi1 - lo1) * cscale * (1.0 + 1e-6));
+            e2 = __double2float_ru(0.5 * (hi2 - lo2) * cscale * (1.0 + 1e-6));
+        }
+        if (lane == 0) {
+            LeafMeta m;
+            m.cx = c0;
+            m.cy = c1;
+            m.cz = c2;
+            m.ipart = ip;
+            m.npart = np;
+            m.hx = LOCAL ? e0 : 1e30f;  // global frames: never claim an entry fully inside
+            m.hy = LOCAL ? e1 : 1e30f;
+            m.hz = LOCAL ? e2 : 1e30f;
+            m.pad = 0.f;
+            meta[l] = m;
+        }
+        for (int q = lane; q < np; q += 32) {
+            const int i = ip + q;
+            pos4[i] = make_float4((float)((X[i] - c0) * cscale), (float)((Y[i] - c1) * cscale),
+                                  (float)((Z[i] - c2) * cscale), mass ? (float)mass[i] : 1.0f);
+        }
+    }
+}
+
+// FP64 form: leaf table only (positions stay FP64 SoA).
+__global__ void prep_plain_kernel(const int *__restrict__ leaf_ip, const int *__restrict__ leaf_np,
+                                  int npart, int nleaf, LeafMeta *__restrict__ meta,
+                                  int *__restrict__ status) {
+    for (int l = blockIdx.x * blockDim.x + threadIdx.x; l < nleaf; l += gridDim.x * blockDim.x) {
+        int ip = leaf_ip[l], np = leaf_np[l];
+        if (!(ip >= 0 && np >= 0 && (int64_t)ip + np <= npart)) {
+            atomicOr(status, ST_LEAF_RANGE);
+            ip = 0;
+            np = 0;
+        }
+        LeafMeta m;
+        m.cx = m.cy = m.cz = 0.0;
+        m.ipart = ip;
+        m.npart = np;
+        m.hx = m.hy = m.hz = m.pad = 0.f;
+        meta[l] = m;
+    }
+}
+
+// ----------------------------------------------------------------- CSR ----
+
+__global__ void csr_count_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
+                                 int nleaf, const LeafMeta *__restrict__ meta,
+                                 int *__restrict__ counts, unsigned long long *__restrict__ pairs,
+                                 int *__restrict__ status) {
+    __shared__ unsigned long long block_pairs;
+    if (threadIdx.x == 0) block_pairs = 0;
+    __syncthreads();
+    unsigned long long local = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        const int t = tt[e], s = ts[e];
+        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) {
+            atomicOr(status, ST_TASK_RANGE);
+            continue;
+        }
+        atomicAdd(&counts[t], 1);
+        local += (unsigned long long)meta[t].npart * (unsigned long long)meta[s].npart;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(kFull, local, off);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(&block_pairs, local);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_pairs) atomicAdd(pairs, block_pairs);
+}
+
+__global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
+                                   int nleaf, const int64_t *__restrict__ row_off,
+                                   int *__restrict__ fill, int *__restrict__ row_src) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        const int t = tt[e], s = ts[e];
+        if ((unsigned)t >= (unsigned)nleaf || (unsigned)s >= (unsigned)nleaf) continue;
+        const int k = atomicAdd(&fill[t], 1);
+        row_src[row_off[t] + k] = s;
+    }
+}
+
+// Rows are sorted by source leaf id after the scatter, so the order in which
+// a row's sources are summed does not depend on the order the atomics
+// placed them in: results are bit-for-bit repeatable.
+//
+// Sorting network: bitonic with "flip" merges, every comparator putting the
+// smaller key at the lower index. Padding a row of length L to the next power
+// of two with +inf keys then never moves a padded key below L, so comparators
+// whose upper index is >= L are simply skipped and no padding is stored.
+template <class Sync>
+__device__ __forceinline__ void flip_bitonic_sort(int *v, int len, int tid, int nthreads,
+                                                  Sync sync) {
+    int P = 1;
+    while (P < len) P <<= 1;
+    for (int size = 2; size <= P; size <<= 1) {
+        const int half = size >> 1;
+        for (int i = tid; i < P / 2; i += nthreads) {
+            const int blk = i / half, off = i % half;
+            const int lo = blk * size + off, hi = blk * size + size - 1 - off;
+            if (hi < len) {
+                const int a = v[lo], b = v[hi];
+                if (a > b) { v[lo] = b; v[hi] = a; }
+            }
+        }
+        sync();
+        for (int stride = half >> 1; stride >= 1; stride >>= 1) {
+            for (int i = tid; i < P / 2; i += nthreads) {
+                const int lo = (i / stride) * 2 * stride + (i % stride), hi = lo + stride;
+                if (hi < len) {
+                    const int a = v[lo], b = v[hi];
+                    if (a > b) { v[lo] = b; v[hi] = a; }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+constexpr int kSortWarpMax = 1024;   // rows up to this length: one warp, shared memory
+constexpr int kSortBlockMax = 8192;  // rows up to this length: one block, shared memory
+constexpr int kSortBlockThreads = 512;
+
+// Rows of length 2..kSortWarpMax, one warp per row (4 warps per block).
+__global__ void __launch_bounds__(128)
+csr_sort_rows_warp_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    __shared__ int buf[4][kSortWarpMax];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *v = buf[w];
+    const int nw = gridDim.x * 4;
+    for (int r = blockIdx.x * 4 + w; r < nleaf; r += nw) {
+        const int64_t b = row_off[r];
+        const int len = (int)(row_off[r + 1] - b);
+        if (len < 2 || len > kSortWarpMax) continue;
+        for (int i = lane; i < len; i += 32) v[i] = row_src[b + i];
+        __syncwarp();
+        flip_bitonic_sort(v, len, lane, 32, []() { __syncwarp(); });
+        for (int i = lane; i < len; i += 32) row_src[b + i] = v[i];
+        __syncwarp();
+    }
+}
+
+// Rows of length kSortWarpMax+1..kSortBlockMax, one block per row.
+__global__ void __launch_bounds__(kSortBlockThreads)
+csr_sort_rows_block_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    __shared__ int v[kSortBlockMax];
+    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
+        const int64_t b = row_off[r];
+        const int len = (int)(row_off[r + 1] - b);
+        if (len <= kSortWarpMax || len > kSortBlockMax) continue;
+        for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = row_src[b + i];
+        __syncthreads();
+        flip_bitonic_sort(v, len, threadIdx.x, blockDim.x, []() { __syncthreads(); });
+        for (int i = threadIdx.x; i < len; i += blockDim.x) row_src[b + i] = v[i];
+        __syncthreads();
+    }
+}
+
+// Longer rows, one block per row, sorted in place in global memory.
+__global__ void __launch_bounds__(kSortBlockThreads)
+csr_sort_rows_global_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
+    for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
+        const int64_t b = row_off[r];
+        const int64_t len = row_off[r + 1] - b;
+        if (len <= kSortBlockMax) continue;
+        __syncthreads();
+        flip_bitonic_sort(row_src + b, (int)len, threadIdx.x, blockDim.x,
+                          []() { __threadfence_block(); __syncthreads(); });
+    }
+}
+
+// Exclusive scan int32 -> int64 in three kernels. kScanTile elements per block.
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t *warp_sums,
+                                                        int64_t *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int64_t y = __shfl_up_sync(kFull, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t ws = lane < (kScanThreads / 32) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int64_t y = __shfl_up_sync(kFull, ws, off);
+            if (lane >= off) ws += y;
+        }
+        if (lane < (kScanThreads / 32)) warp_sums[lane] = ws;
+    }
+    __syncthreads();
+    const int64_t before = (w > 0 ? warp_sums[w - 1] : 0) + x - v;
+    if (total) *total = warp_sums[kScanThreads / 32 - 1];
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_tiles_kernel(const int *__restrict__ in, int n, int64_t *__restrict__ out,
+                  int64_t *__restrict__ tile_sums) {
+    __shared__ int64_t warp_sums[kScanThreads / 32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
+    int64_t v[kScanPer];
+    int64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k;
+        v[k] = i < n ? in[i] : 0;
+        s += v[k];
+    }
+    int64_t total;
+    int64_t run = block_exclusive_scan(s, warp_sums, &total);
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        const int64_t i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+scan_sums_kernel(int64_t *__restrict__ tile_sums, int ntiles, int64_t *__restrict__ grand_total) {
+    __shared__ int64_t warp_sums[kScanThreads / 32];
+    int64_t carry = 0;
+    for (int b0 = 0; b0 < ntiles; b0 += kScanThreads) {
+        const int i = b0 + threadIdx.x;
+        const int64_t v = i < ntiles ? tile_sums[i] : 0;
+        int64_t total;
+        const int64_t ex = block_exclusive_scan(v, warp_sums, &total);
+        if (i < ntiles) tile_sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *grand_total = carry;
+}
+
+__global__ void scan_add_kernel(int64_t *__restrict__ out, int n,
+                                const int64_t *__restrict__ tile_sums) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tile_sums[i / kScanTile];
+}
+
+// --------------------------------------------------------------- probes ---
+
+// FP32 FFMA throughput: 8 independent dependent chains per thread.
+__global__ void __launch_bounds__(256) fma_probe_kernel(float *out, int iters, float m, float b) {
+    float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            x0 = fmaf(x0, m, b); x1 = fmaf(x1, m, b); x2 = fmaf(x2, m, b); x3 = fmaf(x3, m, b);
+            x4 = fmaf(x4, m, b); x5 = fmaf(x5, m, b); x6 = fmaf(x6, m, b); x7 = fmaf(x7, m, b);
+        }
+    }
+    const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace p2p

@@ -42,6 +42,7 @@ class Params(ctypes.Structure):
         ("stage_sources", ctypes.c_int),
         ("blocks_per_sm", ctypes.c_int),
         ("kernel_variant", ctypes.c_int),
+        ("poly_tol", ctypes.c_double),
     ]
 
 

@@ -32,9 +32,9 @@ def _host(a, dtype):
 
 def make_params(form=FORM_PLAIN_FP64, soft_mode=SOFT_CLAMP, soften=1.0, split_radius=1.0,
                 x_cut=2.8125, mass=1.0, warps_per_block=0, stage_sources=0, blocks_per_sm=0,
-                kernel_variant=0):
+                kernel_variant=0, poly_tol=0.0):
     return Params(form, soft_mode, soften, split_radius, x_cut, mass, warps_per_block,
-                  stage_sources, blocks_per_sm, kernel_variant)
+                  stage_sources, blocks_per_sm, kernel_variant, poly_tol)
 
 
 def params_for(cfg, form, mass):
