@@ -76,6 +76,7 @@ struct p2p_session {
     // device buffers
     DevBuf pos, mass, leaf_ip, leaf_np, task_t, task_s, meta, pos4, counts, fill, row_off,
         row_src, tile_sums, acc, status, queue, pairs, probe;
+    DevBuf keys_a, keys_b, vals_b, hist, hoffs, hsums;  // radix sort of the list
     // pass state
     bool in_pass = false;
     int npart = 0, nleaf = 0;
@@ -280,13 +281,62 @@ PairArgs make_args(p2p_session *s) {
     return a;
 }
 
+// Row array of the CSR: the list sorted by sink id with a stable LSD radix
+// sort, its source ids written to row_src.
+int enqueue_radix(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s) {
+    const int nleaf = s->nleaf;
+    int bits = 1;
+    while (bits < 31 && ((int64_t)1 << bits) <= (int64_t)nleaf) ++bits;  // keys in [0, nleaf]
+    const int passes = (bits + 7) / 8;
+    const int ntiles = (int)((ntask + kRadixTile - 1) / kRadixTile);
+    const int nh = kRadixBins * ntiles;
+    const int hscan_tiles = (nh + kScanTile - 1) / kScanTile;
+    int *hist = (int *)s->hist.p;
+    int64_t *hoffs = (int64_t *)s->hoffs.p;
+    int64_t *hsums = (int64_t *)s->hsums.p;
+    int *kbuf[2] = {(int *)s->keys_a.p, (int *)s->keys_b.p};
+    int *vbuf[2] = {(int *)s->row_src.p, (int *)s->vals_b.p};
+    const int *kin = nullptr, *vin = nullptr;
+    for (int pass = 0; pass < passes; ++pass) {
+        const int shift = 8 * pass;
+        const int o = (passes - 1 - pass) & 1;  // the last pass lands in row_src
+        int *kout = pass == passes - 1 ? nullptr : kbuf[o];
+        int *vout = vbuf[o];
+        radix_hist_kernel<<<ntiles, kRadixWarps * 32, 0, s->stream>>>(kin, d_t, d_s, nleaf, ntask, shift,
+                                                                      hist, ntiles);
+        scan_tiles_kernel<<<hscan_tiles, kScanThreads, 0, s->stream>>>(hist, nh, hoffs, hsums);
+        scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>(hsums, hscan_tiles, hoffs + nh);
+        scan_add_kernel<<<grid_for(nh, 256, 1 << 30), 256, 0, s->stream>>>(hoffs, nh, hsums);
+        radix_scatter_kernel<<<ntiles, kRadixWarps * 32, 0, s->stream>>>(
+            kin, vin, d_t, d_s, nleaf, ntask, shift, hoffs, ntiles, kout, vout);
+        CUDA_TRY(cudaGetLastError());
+        launch_count(5);
+        kin = kout;
+        vin = vout;
+    }
+    return P2P_OK;
+}
+
+int size_radix_buffers(p2p_session *s, int64_t ntask) {
+    const size_t n = (size_t)std::max<int64_t>(ntask, 1);
+    const size_t ntiles = (n + kRadixTile - 1) / kRadixTile;
+    const size_t nh = (size_t)kRadixBins * ntiles;
+    P2P_TRY(ensure(s, s->row_src, sizeof(int) * n));
+    P2P_TRY(ensure(s, s->keys_a, sizeof(int) * n));
+    P2P_TRY(ensure(s, s->keys_b, sizeof(int) * n));
+    P2P_TRY(ensure(s, s->vals_b, sizeof(int) * n));
+    P2P_TRY(ensure(s, s->hist, sizeof(int) * nh));
+    P2P_TRY(ensure(s, s->hoffs, sizeof(int64_t) * (nh + 1)));
+    P2P_TRY(ensure(s, s->hsums, sizeof(int64_t) * ((nh + kScanTile - 1) / kScanTile + 1)));
+    return P2P_OK;
+}
+
 // CSR build + pair kernel for one list chunk already on the device.
 int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed) {
     if (ntask <= 0 || s->nleaf <= 0) return P2P_OK;
     const int nleaf = s->nleaf;
     const int threads = 256;
     CUDA_TRY(cudaMemsetAsync(s->counts.p, 0, sizeof(int) * (size_t)nleaf, s->stream));
-    CUDA_TRY(cudaMemsetAsync(s->fill.p, 0, sizeof(int) * (size_t)nleaf, s->stream));
     const int eblocks = grid_for(ntask, threads, 148 * 16);
     csr_count_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf,
                                                          (const LeafMeta *)s->meta.p,
@@ -303,18 +353,8 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
     scan_add_kernel<<<grid_for(nleaf, threads, 1 << 30), threads, 0, s->stream>>>(row_off, nleaf,
                                                                                   tiles);
     CUDA_TRY(cudaGetLastError());
-    csr_scatter_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf, row_off,
-                                                           (int *)s->fill.p, (int *)s->row_src.p);
-    CUDA_TRY(cudaGetLastError());
-    const int sort_blocks = s->sm_count * 8;
-    csr_sort_rows_warp_kernel<<<grid_for((int64_t)nleaf, 4, sort_blocks), 128, 0, s->stream>>>(
-        row_off, nleaf, (int *)s->row_src.p);
-    csr_sort_rows_block_kernel<<<grid_for((int64_t)nleaf, 1, s->sm_count * 2), kSortBlockThreads, 0,
-                                 s->stream>>>(row_off, nleaf, (int *)s->row_src.p);
-    csr_sort_rows_global_kernel<<<grid_for((int64_t)nleaf, 1, s->sm_count), kSortBlockThreads, 0,
-                                  s->stream>>>(row_off, nleaf, (int *)s->row_src.p);
-    CUDA_TRY(cudaGetLastError());
-    launch_count(8);
+    launch_count(4);
+    P2P_TRY(enqueue_radix(s, ntask, d_t, d_s));
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
     // Inside a stream capture the kernel's events become external event-record
@@ -441,7 +481,8 @@ P2P_API int p2p_session_destroy(p2p_session *s) {
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     DevBuf *bufs[] = {&s->pos, &s->mass, &s->leaf_ip, &s->leaf_np, &s->task_t, &s->task_s,
                       &s->meta, &s->pos4, &s->counts, &s->fill, &s->row_off, &s->row_src,
-                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->probe};
+                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->probe,
+                      &s->keys_a, &s->keys_b, &s->vals_b, &s->hist, &s->hoffs, &s->hsums};
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
     cudaEvent_t evs[] = {s->ev_begin, s->ev_end, s->ev_k0, s->ev_k1};
@@ -546,7 +587,7 @@ P2P_API int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, co
     if (!task_t || !task_s) return fail(P2P_ERR_ARG, "null task list");
     P2P_TRY(ensure(s, s->task_t, sizeof(int) * (size_t)ntask));
     P2P_TRY(ensure(s, s->task_s, sizeof(int) * (size_t)ntask));
-    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)ntask));
+    P2P_TRY(size_radix_buffers(s, ntask));
     CUDA_TRY(cudaMemcpyAsync(s->task_t.p, task_t, sizeof(int) * (size_t)ntask, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemcpyAsync(s->task_s.p, task_s, sizeof(int) * (size_t)ntask, cudaMemcpyHostToDevice, s->stream));
     return enqueue_chunk(s, ntask, (const int *)s->task_t.p, (const int *)s->task_s.p, true);
@@ -559,7 +600,7 @@ P2P_API int p2p_pass_submit_device(p2p_session *s, int64_t ntask, const int *d_t
     if (ntask < 0) return fail(P2P_ERR_ARG, "negative ntask");
     if (ntask == 0) return P2P_OK;
     if (!d_task_t || !d_task_s) return fail(P2P_ERR_ARG, "null task list");
-    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)ntask));
+    P2P_TRY(size_radix_buffers(s, ntask));
     return enqueue_chunk(s, ntask, d_task_t, d_task_s, true);
 }
 
@@ -638,7 +679,7 @@ P2P_API int p2p_pass_run_device(p2p_session *s, int npart, const double *d_pos,
     key.version = s->version;
     // sizing may drop a cached graph (buffers moved)
     P2P_TRY(size_pass_buffers(s, npart, nleaf, false, false));
-    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)std::max<int64_t>(ntask, 1)));
+    P2P_TRY(size_radix_buffers(s, ntask));
     s->npart = npart;
     s->nleaf = nleaf;
     s->d_pos = d_pos;

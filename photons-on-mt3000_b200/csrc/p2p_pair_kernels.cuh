@@ -373,8 +373,11 @@ struct SinkPair {
 #ifndef P2P_X2_GROUP
 #define P2P_X2_GROUP 4  // packed sink pairs per predicated block (8 sinks)
 #endif
+#ifndef P2P_X2_SCALAR_POLY
+#define P2P_X2_SCALAR_POLY 0  // 1: polynomial as two scalar Horner chains (measured slower)
+#endif
 #ifndef P2P_X2_ESTRIN
-#define P2P_X2_ESTRIN 1  // polynomial by Estrin's scheme (1) or Horner's rule (0)
+#define P2P_X2_ESTRIN 0  // otherwise packed: Estrin's scheme (1) or Horner's rule (0)
 #endif
 #ifndef P2P_X2_MINBLOCKS
 #define P2P_X2_MINBLOCKS 3  // resident 128-thread blocks per SM the register budget targets
@@ -388,7 +391,16 @@ constexpr int kPairGroup = P2P_X2_GROUP;
 // to about log2(NC) + 1.
 template <int NC>
 __device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
-#if P2P_X2_ESTRIN
+#if P2P_X2_SCALAR_POLY
+    // two scalar Horner chains: coefficients stay constant-bank operands
+    float hx = a.coef[NC - 1], hy = a.coef[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) {
+        hx = fmaf(hx, t.x, a.coef[k]);
+        hy = fmaf(hy, t.y, a.coef[k]);
+    }
+    return make_float2(hx, hy);
+#elif P2P_X2_ESTRIN
     constexpr int NQ = (NC + 1) / 2;  // first-layer terms
     float2 q[NQ];
 #pragma unroll
@@ -427,21 +439,22 @@ __device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
 template <int SOFT, bool MASSES, int NC, bool CHECK>
 __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
                                               const float sw, const SinkPair &p,
-                                              const PairArgs &a, float2 &ax, float2 &ay,
+                                              const PairArgs &a, const float2 eps2v,
+                                              const float2 negu0v, float2 &ax, float2 &ay,
                                               float2 &az, bool &amb) {
     const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
     const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
     const float2 dz = __fadd2_rn(sz, p.z);
     float2 u;
     if (SOFT == SOFT_PLUMMER) {
-        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, make_float2(a.eps2, a.eps2))));
+        u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2v)));
     } else {
         u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
         u.x = fmaxf(u.x, a.eps2);
         u.y = fmaxf(u.y, a.eps2);
     }
     const float2 r = make_float2(rsqrt_approx(u.x), rsqrt_approx(u.y));
-    const float2 t = __fadd2_rn(u, make_float2(-a.u0, -a.u0));
+    const float2 t = __fadd2_rn(u, negu0v);
     const float2 h = poly_x2<NC>(t, a);  // -H(u)
     float2 f = __ffma2_rn(__fmul2_rn(r, r), r, h);
     if (CHECK) {
@@ -499,6 +512,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
     float4 *corr = region + 32;
     float4 *stage = region + 64;
     int *sidx = reinterpret_cast<int *>(stage + stage_cap);
+    const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1);
@@ -560,8 +574,8 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                             if (2 * g < ns) {
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
-                                    pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, src.w, sinks[g + q], a,
-                                                                          ax[g + q], ay[g + q], az[g + q], amb);
+                                    pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
+                                                                          negu0v, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     } else {
@@ -570,8 +584,8 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                             if (2 * g < ns) {
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
-                                    pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, src.w, sinks[g + q], a,
-                                                                           ax[g + q], ay[g + q], az[g + q], amb);
+                                    pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
+                                                                           negu0v, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     }
