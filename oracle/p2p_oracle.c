@@ -197,11 +197,16 @@ int64_t oracle_pair_count(const int *leaf_npart, int64_t ntask, const int *task_
 /*
  * FP64 direct oracle: for each requested sink particle, the sum over ALL
  * particles j != i of the same truncated pair kernel, with minimum-image
- * separations in a periodic cube of side box (box <= 0: open boundaries),
- * using a cell list of cell side >= r_cut = 2 r_s x_cut. Independent of the
- * tree and lists; comparable to the list-based pass when the lists hold every
- * leaf pair within r_cut and there are no ghost particles. pos is SoA over the
- * n particles of the box; out is SoA over the nsink requested sinks.
+ * separations in a periodic cube of side box (box <= 0: open boundaries).
+ * Independent of the tree and lists; comparable to the list-based pass when
+ * the lists hold every leaf pair within r_cut = 2 r_s x_cut and there are no
+ * ghost particles. pos is SoA over the n particles of the box; out is SoA
+ * over the nsink requested sinks.
+ *
+ * Candidates come from a cell list of cell side >= r_cut / 2 (5^3 cells
+ * around the sink's), with the positions copied into cell order so the scan
+ * is sequential; candidates farther than r_cut are rejected on r^2 before
+ * the pair function (which makes the exact cutoff decision) is called.
  */
 void oracle_direct(const oracle_params *p, int n, const double *pos,
                    const double *masses, double box, int nsink, const int *sinks,
@@ -212,8 +217,9 @@ void oracle_direct(const oracle_params *p, int n, const double *pos,
     const double r_soft = 1.0 / p->soften;
     const double r_cut = 2.0 * p->split_radius * p->x_cut;
     const double *X = pos, *Y = pos + n, *Z = pos + 2 * (size_t)n;
+    const int wrap = box > 0;
     double lo[3] = {0, 0, 0}, span = box;
-    if (box <= 0.0) {
+    if (!wrap) {
         double hi[3] = {X[0], Y[0], Z[0]};
         lo[0] = X[0]; lo[1] = Y[0]; lo[2] = Z[0];
         for (int i = 0; i < n; ++i) {
@@ -239,7 +245,8 @@ void oracle_direct(const oracle_params *p, int n, const double *pos,
         }
         lo[0] = lo[1] = lo[2] = floor(mn / box) * box;
     }
-    int nc = (int)floor(span / r_cut);
+    /* r_cut <= 0 (no per-pair cutoff) makes every particle a candidate */
+    int nc = r_cut > 0.0 ? (int)floor(span / (0.5 * r_cut)) : 1;
     if (nc < 1) nc = 1;
     if (nc > 256) nc = 256;
     const double cw = span / nc;
@@ -252,7 +259,7 @@ void oracle_direct(const oracle_params *p, int n, const double *pos,
         const double q[3] = {X[i], Y[i], Z[i]};
         for (int d = 0; d < 3; ++d) {
             double v = q[d] - lo[d];
-            if (box > 0) v = fmod(fmod(v, box) + box, box);
+            if (wrap) v = fmod(fmod(v, box) + box, box);
             int k = (int)floor(v / cw);
             c[d] = k < 0 ? 0 : (k >= nc ? nc - 1 : k);
         }
@@ -266,17 +273,27 @@ void oracle_direct(const oracle_params *p, int n, const double *pos,
         for (int i = 0; i < n; ++i) order[cur[cell_of[i]]++] = i;
         free(cur);
     }
-    const int reach = (int)ceil(r_cut / cw);
-#pragma omp parallel for schedule(dynamic, 64)
+    /* positions (and masses) in cell order */
+    double *cx = (double *)malloc(sizeof(double) * (size_t)n * 4);
+    double *cy = cx + n, *cz = cx + 2 * (size_t)n, *cm = cx + 3 * (size_t)n;
+    for (int q = 0; q < n; ++q) {
+        const int j = order[q];
+        cx[q] = X[j]; cy[q] = Y[j]; cz[q] = Z[j];
+        cm[q] = masses ? masses[j] : 1.0;
+    }
+    const int reach = r_cut > 0.0 ? (int)ceil(r_cut / cw) : nc;
+    /* candidates beyond this cannot pass the pair's own cutoff test */
+    const double reject2 = r_cut > 0.0 ? r_cut * r_cut * (1.0 + 1e-9) : INFINITY;
+    const double hb = 0.5 * box;
+#pragma omp parallel for schedule(dynamic, 1)
     for (int s = 0; s < nsink; ++s) {
-        int i = sinks[s];
-        int ci = cell_of[i];
-        int c0 = ci / (nc * nc), c1 = (ci / nc) % nc, c2 = ci % nc;
-        double ii[3] = {X[i], Y[i], Z[i]};
+        const int i = sinks[s];
+        const int ci = cell_of[i];
+        const int c0 = ci / (nc * nc), c1 = (ci / nc) % nc, c2 = ci % nc;
+        const double ii[3] = {X[i], Y[i], Z[i]};
         double a[3] = {0, 0, 0};
         int lim = reach;
         int span_cells = 2 * lim + 1;
-        int wrap = box > 0;
         if (span_cells > nc) { lim = nc / 2; span_cells = nc; }
         for (int a0 = -lim; a0 < -lim + span_cells; ++a0)
             for (int a1 = -lim; a1 < -lim + span_cells; ++a1)
@@ -287,34 +304,39 @@ void oracle_direct(const oracle_params *p, int n, const double *pos,
                     } else if (k0 < 0 || k1 < 0 || k2 < 0 || k0 >= nc || k1 >= nc || k2 >= nc) {
                         continue;
                     }
-                    int64_t cc = ((int64_t)k0 * nc + k1) * nc + k2;
+                    const int64_t cc = ((int64_t)k0 * nc + k1) * nc + k2;
                     for (int64_t q = cstart[cc]; q < cstart[cc + 1]; ++q) {
-                        int j = order[q];
-                        if (j == i) continue;
-                        double jj[3] = {X[j], Y[j], Z[j]};
+                        double dd[3] = {cx[q] - ii[0], cy[q] - ii[1], cz[q] - ii[2]};
                         if (wrap) {
                             for (int d = 0; d < 3; ++d) {
-                                double dd = jj[d] - ii[d];
-                                dd -= box * nearbyint(dd / box);
-                                jj[d] = ii[d] + dd;
+                                /* minimum image: dd - box * nearbyint(dd / box) */
+                                if (dd[d] > hb || dd[d] < -hb) {
+                                    if (dd[d] < 3.0 * hb && dd[d] > -3.0 * hb)
+                                        dd[d] += dd[d] > 0 ? -box : box;
+                                    else
+                                        dd[d] -= box * nearbyint(dd[d] / box);
+                                }
                             }
                         }
+                        if (dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2] > reject2) continue;
+                        if (order[q] == i) continue;
+                        const double jj[3] = {ii[0] + dd[0], ii[1] + dd[1], ii[2] + dd[2]};
                         double one[3] = {0, 0, 0};
                         if (p->soft_mode == ORACLE_SOFT_PLUMMER)
                             pair_plummer(p->soften, rrs, coeff, p->x_cut, ii, jj, one);
                         else
                             pair_clamp(p->soften, r_soft, hrrs, coeff, p->x_cut, ii, jj, one);
-                        double m = masses ? masses[j] : 1.0;
-                        a[0] += m * one[0];
-                        a[1] += m * one[1];
-                        a[2] += m * one[2];
+                        a[0] += cm[q] * one[0];
+                        a[1] += cm[q] * one[1];
+                        a[2] += cm[q] * one[2];
                     }
                 }
-        double m = masses ? 1.0 : p->mass;
+        const double m = masses ? 1.0 : p->mass;
         out[s] = a[0] * m;
         out[nsink + s] = a[1] * m;
         out[2 * (size_t)nsink + s] = a[2] * m;
     }
+    free(cx);
     free(cstart);
     free(cell_of);
     free(order);

@@ -284,6 +284,7 @@ inline int acceptance(const double wi[3], const double wj[3], const double dist[
 struct Walker {
     const Tree &T;
     double cutoff, open_angle;
+    const std::vector<char> *node_has_sink;  // null: no pruning
     int defer_depth;                 // < 0: never defer
     std::vector<int> *out_t, *out_s; // emitted (sink, source) leaf ids
     std::vector<int64_t> *deferred;  // packed (im, jm) deferred calls, in order
@@ -303,6 +304,8 @@ struct Walker {
     }
     // walk_task_p2p, src/fmm.c:656-792.
     void walk(int im, int jm, int depth) {
+        // a sink-side subtree without an active leaf emits nothing: skip it
+        if (node_has_sink && is_node(im) && !(*node_has_sink)[cidx(im)]) return;
         if (defer_depth >= 0 && depth >= defer_depth && (is_node(im) || is_node(jm))) {
             seq->push_back((int64_t)deferred->size());
             deferred->push_back(((int64_t)im << 32) | (uint32_t)jm);
@@ -507,9 +510,45 @@ void p2p_tree_leaves(const p2p_tree *h, int *ipart, int *npart, int *active, dou
     }
 }
 
+namespace {
+// has_sink[node] = the subtree holds a leaf with active >= 0
+char mark_sinks(const Tree &T, int c, std::vector<char> &has) {
+    if (!is_node(c)) return T.leaves[cidx(c)].active >= 0;
+    const Node &n = T.nodes[cidx(c)];
+    const char a = mark_sinks(T, n.son[0], has);
+    const char b = mark_sinks(T, n.son[1], has);
+    return has[cidx(c)] = (char)(a || b);
+}
+int64_t walk_impl(p2p_tree *h, double cutoff, double open_angle, const std::vector<char> *prune);
+}  // namespace
+
 // Runs the P2P walk from (root, root). Returns the number of list entries
 // kept inside the handle (fetch them with p2p_tree_tasks).
 int64_t p2p_tree_walk(p2p_tree *h, double cutoff, double open_angle) {
+    return walk_impl(h, cutoff, open_angle, nullptr);
+}
+
+// The walk restricted to the sink leaves with sink_mask[leaf] != 0 (others
+// are treated as inactive sinks, like ghost-only leaves). The emitted entries
+// are exactly the unrestricted walk's entries whose sink is kept, in the
+// same order; subtrees without a kept sink are not descended into.
+int64_t p2p_tree_walk_masked(p2p_tree *h, double cutoff, double open_angle,
+                             const unsigned char *sink_mask) {
+    Tree &T = h->T;
+    std::vector<int> saved(T.leaves.size());
+    for (size_t l = 0; l < T.leaves.size(); ++l) {
+        saved[l] = T.leaves[l].active;
+        if (!sink_mask[l]) T.leaves[l].active = -1;
+    }
+    std::vector<char> has(T.nodes.size(), 0);
+    mark_sinks(T, 1, has);
+    const int64_t n = walk_impl(h, cutoff, open_angle, &has);
+    for (size_t l = 0; l < T.leaves.size(); ++l) T.leaves[l].active = saved[l];
+    return n;
+}
+
+namespace {
+int64_t walk_impl(p2p_tree *h, double cutoff, double open_angle, const std::vector<char> *prune) {
     const Tree &T = h->T;
     h->task_t.clear();
     h->task_s.clear();
@@ -523,14 +562,14 @@ int64_t p2p_tree_walk(p2p_tree *h, double cutoff, double open_angle) {
     int depth = 12;
     if (nthreads > 1) depth = 16;
     {
-        Walker w{T, cutoff, open_angle, depth, &top_t, &top_s, &deferred, &seq};
+        Walker w{T, cutoff, open_angle, prune, depth, &top_t, &top_s, &deferred, &seq};
         w.walk(root, root, 0);
     }
     std::vector<std::vector<int>> dt(deferred.size()), ds(deferred.size());
 #pragma omp parallel for schedule(dynamic, 4)
     for (size_t k = 0; k < deferred.size(); ++k) {
         int im = (int)(deferred[k] >> 32), jm = (int)(uint32_t)deferred[k];
-        Walker w{T, cutoff, open_angle, -1, &dt[k], &ds[k], nullptr, nullptr};
+        Walker w{T, cutoff, open_angle, prune, -1, &dt[k], &ds[k], nullptr, nullptr};
         w.walk(im, jm, 0);
     }
     // Concatenate in serial order.
@@ -556,6 +595,7 @@ int64_t p2p_tree_walk(p2p_tree *h, double cutoff, double open_angle) {
     }
     return total;
 }
+}  // namespace
 
 void p2p_tree_tasks(const p2p_tree *h, int *task_t, int *task_s) {
     std::memcpy(task_t, h->task_t.data(), sizeof(int) * h->task_t.size());

@@ -50,6 +50,8 @@ def lists():
         lib.p2p_tree_walk.restype = ctypes.c_int64
         lib.p2p_tree_walk.argtypes = [_vp, ctypes.c_double, ctypes.c_double]
         lib.p2p_tree_tasks.argtypes = [_vp, _i32p, _i32p]
+        lib.p2p_tree_walk_masked.restype = ctypes.c_int64
+        lib.p2p_tree_walk_masked.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
         lib.p2p_lists_num_threads.restype = ctypes.c_int
         lib._typed = True
     return lib

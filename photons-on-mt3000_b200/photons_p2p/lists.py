@@ -75,9 +75,11 @@ class TreeLists:
         return int(np.dot(n[self.task_t], n[self.task_s]))
 
 
-def build_tree_lists(pos, tag, maxleaf, boxsize, cutoff, open_angle):
+def build_tree_lists(pos, tag, maxleaf, boxsize, cutoff, open_angle, sink_particles=None):
     """kd-tree (src/fmm.c:231-327) + P2P walk (src/fmm.c:656-792) over the
-    given particles (pos (3, n) float64, tag (n,) int: 1 local, 0 ghost)."""
+    given particles (pos (3, n) float64, tag (n,) int: 1 local, 0 ghost).
+    sink_particles (original indices, optional) keeps only the list rows of
+    the leaves holding them (the same entries, in the same order)."""
     lib = _native.lists()
     pos = np.array(pos, dtype=np.float64, order="C", copy=True)
     tag = np.ascontiguousarray(tag, dtype=np.int32)
@@ -96,7 +98,15 @@ def build_tree_lists(pos, tag, maxleaf, boxsize, cutoff, open_angle):
         wid = np.empty((nleaf, 3), np.float64)
         lib.p2p_tree_leaves(h, _ptr(ip, _i32p), _ptr(npt, _i32p), _ptr(act, _i32p),
                             _ptr(ctr, _f64p), _ptr(wid, _f64p))
-        nt = lib.p2p_tree_walk(h, cutoff, open_angle)
+        if sink_particles is None:
+            nt = lib.p2p_tree_walk(h, cutoff, open_angle)
+        else:
+            slot = np.empty(n, np.int64)
+            slot[perm] = np.arange(n)
+            leaf_of_slot = np.repeat(np.arange(nleaf), npt)
+            mask = np.zeros(nleaf, np.uint8)
+            mask[leaf_of_slot[slot[np.asarray(sink_particles)]]] = 1
+            nt = lib.p2p_tree_walk_masked(h, cutoff, open_angle, mask.ctypes.data_as(ctypes.c_void_p))
         tt = np.empty(nt, np.int32)
         ts = np.empty(nt, np.int32)
         lib.p2p_tree_tasks(h, _ptr(tt, _i32p), _ptr(ts, _i32p))

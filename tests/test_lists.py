@@ -88,3 +88,28 @@ def test_lists_partition_and_symmetry():
     # every active leaf lists itself
     act = np.nonzero(tl.leaf_active >= 0)[0]
     assert all((int(a), int(a)) in pairs for a in act)
+
+
+@pytest.mark.parametrize("nsink", [1, 50, 3000])
+def test_masked_walk_equals_filtered_walk(nsink):
+    """The walk restricted to the leaves of sampled sinks emits exactly the
+    full walk's rows of those leaves, in the same order (with ghosts and a
+    shifted origin, as the precision study uses it)."""
+    cfg = W.scaled(W.c5_config(), n_side=40, mesh=40, eps=1 / (200 * 40))
+    pos = W.c5_positions(40 ** 3)
+    allpos, tag = W.with_ghosts(pos, cfg)
+    full = L.build_tree_lists(allpos, tag, cfg.maxleaf, cfg.box, cfg.cutoff_radius,
+                              cfg.open_angle)
+    sinks = np.random.default_rng(nsink).choice(pos.shape[1], nsink, replace=False)
+    part = L.build_tree_lists(allpos, tag, cfg.maxleaf, cfg.box, cfg.cutoff_radius,
+                              cfg.open_angle, sink_particles=sinks)
+    assert np.array_equal(part.perm, full.perm)
+    slot = np.empty(full.npart, np.int64)
+    slot[full.perm] = np.arange(full.npart)
+    leaf_of = np.repeat(np.arange(full.nleaf), full.leaf_npart)
+    keep = np.zeros(full.nleaf, bool)
+    keep[leaf_of[slot[sinks]]] = True
+    sel = keep[full.task_t]
+    assert sel.any()
+    assert np.array_equal(part.task_t, full.task_t[sel])
+    assert np.array_equal(part.task_s, full.task_s[sel])
