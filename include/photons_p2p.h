@@ -186,6 +186,96 @@ int p2p_pass_noalloc(const p2p_params *params, int npart, const double *d_pos, i
  * dependent-chain microbenchmark run on the session stream. */
 int p2p_measure_fp32_peak(p2p_session *s, double *tflops);
 
+/* ---- Serving an ensemble of boxes (no counterpart in the reference) -----
+ * A server takes force-pass requests for many independent periodic boxes.
+ * Each box's particles, leaf frames and CSR list are built once on the
+ * device and stay resident in an arena of fixed size (hbm_bytes); a box is
+ * admitted when its footprint fits, evicting least recently used idle boxes
+ * when it does not, and otherwise waits until memory frees up. Requests of
+ * different boxes that are pending together are packed into one persistent
+ * pair-kernel launch (up to max_pack boxes); up to `slots` launches are in
+ * flight at once on their own streams, so requests arriving while others run
+ * are admitted as slots and memory free up and run alongside them. A box's
+ * result does not depend on which other boxes share its launch.
+ *
+ * Units. All boxes share the kernel shape `shape` (form, softening mode,
+ * x_cut, poly_tol, kernel variant, and soften / split_radius in shape length
+ * units; shape->mass is ignored). A box is given in its own length unit with
+ * length_scale = (shape length unit) / (box length unit), i.e. box positions
+ * times length_scale are shape positions: a box with split radius r_s and
+ * softening eps uses length_scale = shape->split_radius / r_s and then has
+ * eps = shape->soften / length_scale. Its result is in box units with the
+ * box's equal particle mass `mass`. */
+typedef struct p2p_server p2p_server;
+
+typedef struct {
+    int slots;                 /* packed launches in flight at once; 0: 1 (measured best
+                                  throughput; results still drain on a copy stream while
+                                  the next launch computes) */
+    int max_pack;              /* boxes per launch, 1..32; 0: 32 */
+    int full_grid;             /* 0: each launch takes 1/slots of the GPU's resident
+                                  blocks; 1 (default): every launch takes all of them */
+    size_t hbm_bytes;          /* device memory for resident boxes; 0: half the free memory */
+    double rows_per_particle;  /* arena split hint: list entries per particle; 0: 24 */
+    double particles_per_leaf; /* arena split hint; 0: 16 */
+} p2p_server_config;
+
+typedef struct {
+    int64_t requests_done;
+    int64_t launches;          /* packed pair-kernel launches */
+    int64_t boxes_launched;    /* sum over launches of boxes packed */
+    int64_t builds;            /* residency builds (first admission or re-admission) */
+    int64_t evictions;
+    int64_t pairs;             /* pair interactions computed */
+    double kernel_ms;          /* sum over launches of pair-kernel time (CUDA events) */
+    double build_ms;           /* sum over builds of their device time */
+    int resident_boxes;
+    size_t resident_bytes, capacity_bytes;
+} p2p_server_stats;
+
+void p2p_server_config_default(p2p_server_config *cfg);
+int p2p_server_create(int device, const p2p_params *shape, const p2p_server_config *cfg,
+                      p2p_server **out);
+/* Waits for every submitted request, then frees everything. */
+int p2p_server_destroy(p2p_server *srv);
+/* Registers a box (nothing is copied yet). pos: 3*npart doubles, SoA, in the
+ * box's tree order; leaf ranges and the (sink, source) list as for
+ * p2p_pass_begin / p2p_pass_submit. result_slots (nresult particle slots,
+ * may be NULL) selects and orders the particles whose accelerations a
+ * request returns, e.g. the local particles in their original order without
+ * the ghosts; NULL returns every particle in slot order (nresult ignored).
+ * The host arrays are read whenever the box is (re)admitted and must stay
+ * valid and unchanged until the server is destroyed. Checks every range
+ * (P2P_ERR_RANGE) and that the box fits in the arena at all
+ * (P2P_ERR_CAPACITY). Preloaded boxes (p2p_server_preload) are exempt from
+ * the lifetime rule once that call has returned. */
+int p2p_server_add_box(p2p_server *srv, double length_scale, double mass, int npart,
+                       const double *pos, int nleaf, const int *leaf_ipart, const int *leaf_npart,
+                       int64_t ntask, const int *task_t, const int *task_s, int nresult,
+                       const int *result_slots, int *box_id);
+/* Makes the box resident now and pins it (never evicted); after it returns
+ * the box's host arrays are no longer read and may be freed. Returns
+ * P2P_ERR_CAPACITY if it cannot fit beside the pinned and queued boxes. */
+int p2p_server_preload(p2p_server *srv, int box_id);
+/* Device bytes the box holds while resident. */
+int p2p_server_box_bytes(p2p_server *srv, int box_id, size_t *bytes);
+/* Queues one force pass of the box. out: 3*nresult doubles (3*npart without
+ * a result map) of page-locked host memory (p2p_host_alloc, cudaHostAlloc or
+ * cudaHostRegister), SoA, overwritten with the selected particles'
+ * accelerations in box units. */
+int p2p_server_submit(p2p_server *srv, int box_id, double *out, int64_t *ticket);
+/* Blocks until the request's result is in `out`; latency_s (may be null) is
+ * the time from its submit to that moment. */
+int p2p_server_wait(p2p_server *srv, int64_t ticket, double *latency_s);
+/* Non-blocking: *done = 1 and the latency once the result is in `out`. */
+int p2p_server_query(p2p_server *srv, int64_t ticket, int *done, double *latency_s);
+/* Blocks until every submitted request has finished. */
+int p2p_server_drain(p2p_server *srv);
+int p2p_server_get_stats(p2p_server *srv, p2p_server_stats *stats);
+/* Page-locked, device-mapped host memory for server results. */
+int p2p_host_alloc(size_t bytes, void **ptr);
+int p2p_host_free(void *ptr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,8 +16,14 @@
 #include "photons_p2p.h"
 #include "p2p_internal.h"
 #include "p2p_fit.h"
+#include "p2p_args.h"
 #include "p2p_launch.h"
+#include "p2p_host_shared.h"
 #include "p2p_pass_kernels.cuh"
+
+namespace p2p {
+#include "p2p_csr.h"
+}  // namespace p2p
 
 #define P2P_API extern "C" __attribute__((visibility("default")))
 
@@ -259,102 +265,42 @@ PairArgs make_args(p2p_session *s) {
     a.queue = (int *)s->queue.p;
     a.npart = s->npart;
     a.nleaf = s->nleaf;
-    const double c = 0.5 / p.split_radius;
-    a.cscale = c;
-    a.eps2 = (float)((c * p.soften) * (c * p.soften));
-    a.u0 = (float)s->fit.u0;
-    a.ucut = (float)s->fit.umax;
-    a.ucut_lo = (float)(s->fit.umax * (1.0 - kCutBand));
-    a.ucut_hi = (float)(s->fit.umax * (1.0 + kCutBand));
-    a.rcut2 = s->fit.umax / (c * c);
-    a.eps2_box = p.soften * p.soften;
-    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = -s->fit.coef[k];
-    a.uin = (float)(s->fit.umax * (1.0 - kInsideMargin));
-    a.out_scale = c * c * (s->d_mass ? 1.0 : p.mass);
-    a.soft = p.soften;
-    a.r_soft = 1.0 / p.soften;
-    a.rrs = 1.0 / p.split_radius;
-    a.hrrs = 0.5 * a.rrs;
-    a.coeff = 2.0 * (1.0 / std::sqrt(M_PI));
-    a.xcut = p.x_cut;
-    a.mass_eq = p.mass;
+    fill_pass_scalars(a, p, s->fit, s->d_mass != nullptr);
     return a;
-}
-
-// Row array of the CSR: the list sorted by sink id with a stable LSD radix
-// sort, its source ids written to row_src.
-int enqueue_radix(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s) {
-    const int nleaf = s->nleaf;
-    int bits = 1;
-    while (bits < 31 && ((int64_t)1 << bits) <= (int64_t)nleaf) ++bits;  // keys in [0, nleaf]
-    const int passes = (bits + 7) / 8;
-    const int ntiles = (int)((ntask + kRadixTile - 1) / kRadixTile);
-    const int nh = kRadixBins * ntiles;
-    const int hscan_tiles = (nh + kScanTile - 1) / kScanTile;
-    int *hist = (int *)s->hist.p;
-    int64_t *hoffs = (int64_t *)s->hoffs.p;
-    int64_t *hsums = (int64_t *)s->hsums.p;
-    int *kbuf[2] = {(int *)s->keys_a.p, (int *)s->keys_b.p};
-    int *vbuf[2] = {(int *)s->row_src.p, (int *)s->vals_b.p};
-    const int *kin = nullptr, *vin = nullptr;
-    for (int pass = 0; pass < passes; ++pass) {
-        const int shift = 8 * pass;
-        const int o = (passes - 1 - pass) & 1;  // the last pass lands in row_src
-        int *kout = pass == passes - 1 ? nullptr : kbuf[o];
-        int *vout = vbuf[o];
-        radix_hist_kernel<<<ntiles, kRadixWarps * 32, 0, s->stream>>>(kin, d_t, d_s, nleaf, ntask, shift,
-                                                                      hist, ntiles);
-        scan_tiles_kernel<<<hscan_tiles, kScanThreads, 0, s->stream>>>(hist, nh, hoffs, hsums);
-        scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>(hsums, hscan_tiles, hoffs + nh);
-        scan_add_kernel<<<grid_for(nh, 256, 1 << 30), 256, 0, s->stream>>>(hoffs, nh, hsums);
-        radix_scatter_kernel<<<ntiles, kRadixWarps * 32, 0, s->stream>>>(
-            kin, vin, d_t, d_s, nleaf, ntask, shift, hoffs, ntiles, kout, vout);
-        CUDA_TRY(cudaGetLastError());
-        launch_count(5);
-        kin = kout;
-        vin = vout;
-    }
-    return P2P_OK;
 }
 
 int size_radix_buffers(p2p_session *s, int64_t ntask) {
     const size_t n = (size_t)std::max<int64_t>(ntask, 1);
-    const size_t ntiles = (n + kRadixTile - 1) / kRadixTile;
-    const size_t nh = (size_t)kRadixBins * ntiles;
     P2P_TRY(ensure(s, s->row_src, sizeof(int) * n));
     P2P_TRY(ensure(s, s->keys_a, sizeof(int) * n));
     P2P_TRY(ensure(s, s->keys_b, sizeof(int) * n));
     P2P_TRY(ensure(s, s->vals_b, sizeof(int) * n));
-    P2P_TRY(ensure(s, s->hist, sizeof(int) * nh));
-    P2P_TRY(ensure(s, s->hoffs, sizeof(int64_t) * (nh + 1)));
-    P2P_TRY(ensure(s, s->hsums, sizeof(int64_t) * ((nh + kScanTile - 1) / kScanTile + 1)));
+    P2P_TRY(ensure(s, s->hist, sizeof(int) * csr_hist_len(ntask)));
+    P2P_TRY(ensure(s, s->hoffs, sizeof(int64_t) * (csr_hist_len(ntask) + 1)));
+    P2P_TRY(ensure(s, s->hsums, sizeof(int64_t) * csr_hsum_len(ntask)));
     return P2P_OK;
 }
 
 // CSR build + pair kernel for one list chunk already on the device.
 int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed) {
     if (ntask <= 0 || s->nleaf <= 0) return P2P_OK;
-    const int nleaf = s->nleaf;
-    const int threads = 256;
-    CUDA_TRY(cudaMemsetAsync(s->counts.p, 0, sizeof(int) * (size_t)nleaf, s->stream));
-    const int eblocks = grid_for(ntask, threads, 148 * 16);
-    csr_count_kernel<<<eblocks, threads, 0, s->stream>>>(d_t, d_s, ntask, nleaf,
-                                                         (const LeafMeta *)s->meta.p,
-                                                         (int *)s->counts.p,
-                                                         (unsigned long long *)s->pairs.p,
-                                                         (int *)s->status.p);
-    CUDA_TRY(cudaGetLastError());
-    const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
-    int64_t *row_off = (int64_t *)s->row_off.p;
-    int64_t *tiles = (int64_t *)s->tile_sums.p;
-    scan_tiles_kernel<<<ntiles, kScanThreads, 0, s->stream>>>((const int *)s->counts.p, nleaf,
-                                                              row_off, tiles);
-    scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>(tiles, ntiles, row_off + nleaf);
-    scan_add_kernel<<<grid_for(nleaf, threads, 1 << 30), threads, 0, s->stream>>>(row_off, nleaf,
-                                                                                  tiles);
-    CUDA_TRY(cudaGetLastError());
-    launch_count(4);
-    P2P_TRY(enqueue_radix(s, ntask, d_t, d_s));
+    CsrBufs b;
+    b.counts = (int *)s->counts.p;
+    b.row_off = (int64_t *)s->row_off.p;
+    b.tile_sums = (int64_t *)s->tile_sums.p;
+    b.row_src = (int *)s->row_src.p;
+    b.keys_a = (int *)s->keys_a.p;
+    b.keys_b = (int *)s->keys_b.p;
+    b.vals_b = (int *)s->vals_b.p;
+    b.hist = (int *)s->hist.p;
+    b.hoffs = (int64_t *)s->hoffs.p;
+    b.hsums = (int64_t *)s->hsums.p;
+    b.pairs = (unsigned long long *)s->pairs.p;
+    b.status = (int *)s->status.p;
+    int launched = 0;
+    CUDA_TRY(enqueue_csr_build(s->stream, ntask, d_t, d_s, s->nleaf, (const LeafMeta *)s->meta.p, b,
+                               &launched));
+    launch_count(launched);
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
     // Inside a stream capture the kernel's events become external event-record
@@ -383,8 +329,7 @@ int size_pass_buffers(p2p_session *s, int npart, int nleaf, bool host_inputs, bo
     P2P_TRY(ensure(s, s->counts, sizeof(int) * (size_t)nleaf));
     P2P_TRY(ensure(s, s->fill, sizeof(int) * (size_t)nleaf));
     P2P_TRY(ensure(s, s->row_off, sizeof(int64_t) * ((size_t)nleaf + 1)));
-    const size_t ntiles = ((size_t)nleaf + kScanTile - 1) / kScanTile + 1;
-    P2P_TRY(ensure(s, s->tile_sums, sizeof(int64_t) * ntiles));
+    P2P_TRY(ensure(s, s->tile_sums, sizeof(int64_t) * csr_tile_sums(nleaf)));
     P2P_TRY(ensure(s, s->status, sizeof(int)));
     P2P_TRY(ensure(s, s->queue, sizeof(int)));
     P2P_TRY(ensure(s, s->pairs, sizeof(unsigned long long)));
@@ -405,6 +350,18 @@ int check_session(p2p_session *s) {
 }
 
 }  // namespace
+
+// Host-side services shared with the server's translation unit
+// (p2p_host_shared.h).
+namespace p2p {
+int report_error(int status, const char *msg) {
+    g_last_error = msg;
+    return status;
+}
+int check_params(const p2p_params *p) { return validate_params(p); }
+void count_launches(int n) { g_launches += n; }
+cudaError_t allow_large_smem() { return allow_smem_all(); }
+}  // namespace p2p
 
 // ------------------------------------------------------------------ ABI ---
 

@@ -1,0 +1,18 @@
+// Host services of libphotons_p2p shared across its translation units
+// (defined in p2p_core.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "photons_p2p.h"
+
+namespace p2p {
+// Records msg as p2p_last_error() of the calling thread; returns status.
+int report_error(int status, const char *msg);
+// P2P_OK or P2P_ERR_ARG (with the message recorded) for a parameter set.
+int check_params(const p2p_params *p);
+// Adds to p2p_kernel_launch_count().
+void count_launches(int n);
+// Opts every pair kernel into large dynamic shared memory on the current device.
+cudaError_t allow_large_smem();
+}  // namespace p2p

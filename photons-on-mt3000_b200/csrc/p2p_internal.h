@@ -22,6 +22,7 @@ enum : int {
 };
 
 constexpr int kMaxCoef = 21;  // polynomial degree <= 20
+constexpr int kMaxSeg = 32;   // boxes per packed launch (one warp ballot maps an item)
 
 // Relative half-width of the cutoff band around x_cut^2 inside which FP32
 // rounding of u cannot decide a pair (coordinate rounding bounds the FP32
@@ -64,6 +65,12 @@ struct PairArgs {
     float uin;               // entries whose bound on u stays below uin hold no cutoff-band pair
     // FP64 form (reference units)
     double soft, r_soft, hrrs, rrs, coeff, xcut, mass_eq;
+    // Packed launches over several resident boxes (nseg > 0): work items
+    // [seg_item[k], seg_item[k + 1]) are the sink leaves seg_leaf[k] + 0, 1, ...
+    // of box k; nleaf then counts the items. nseg = 0: item i is leaf i.
+    int nseg;
+    int seg_item[kMaxSeg + 1];
+    int seg_leaf[kMaxSeg];
 };
 
 }  // namespace p2p

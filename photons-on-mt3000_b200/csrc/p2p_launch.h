@@ -26,6 +26,7 @@ struct PairLaunch {
     int blocks_per_sm;  // 0: as many as fit
     bool dry_run;       // resolve the launch shape only
     OccupancyCache *occ;
+    int max_blocks = 0; // > 0: cap on the persistent grid (a share of the GPU)
 };
 
 struct PairLaunchResult {
@@ -63,6 +64,7 @@ bool persistent_blocks(const PairLaunch &L, K kernel, size_t smem, PairLaunchRes
         return false;
     }
     r.blocks = per_sm * L.sm_count;
+    if (L.max_blocks > 0 && r.blocks > L.max_blocks) r.blocks = L.max_blocks;
     return true;
 }
 

@@ -137,6 +137,16 @@ __device__ __forceinline__ void consume_split(const float4 *stage, int fill, int
 
 // Lanes per sink particle group: 32 sink particles per warp pass, or for
 // small slices several lanes share a particle and split its sources.
+// Sink leaf of work item `item` (warp-uniform): the item itself in a pass over
+// one box; in a packed launch, the item's place in the leaf range of the box
+// whose segment holds it (segments start at ascending items, seg_item[0] = 0).
+__device__ __forceinline__ int item_leaf(const PairArgs &a, const int item, const int lane) {
+    if (a.nseg == 0) return item;
+    const unsigned m = __ballot_sync(kFull, lane < a.nseg && a.seg_item[lane] <= item);
+    const int k = 31 - __clz(m);
+    return a.seg_leaf[k] + (item - a.seg_item[k]);
+}
+
 __device__ __forceinline__ int group_size(int ns) { return ns > 16 ? 32 : (ns > 8 ? 16 : 8); }
 
 template <int SOFT, bool MASSES, int ACC, int NC>
@@ -151,9 +161,10 @@ pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
         if (lane == 0) item = atomicAdd(a.queue, 1);
         item = __shfl_sync(kFull, item, 0);
         if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        const int li = item_leaf(a, item, lane);
+        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
         if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
+        const LeafMeta mt = a.leaf[li];
         for (int s0 = 0; s0 < mt.npart; s0 += 32) {
             const int ns = min(32, mt.npart - s0);
             const int gs = group_size(ns);
@@ -225,8 +236,8 @@ pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
 constexpr int kSinkGroup = 4;        // sinks evaluated per predicated block
 constexpr int kSrcFlushChunks = 32;  // FP32 partial depth per lane, in chunks
 
-template <int K>
-__device__ __forceinline__ void butterfly_step(float (&v)[32], const int lane) {
+template <int K, int N>
+__device__ __forceinline__ void butterfly_step(float (&v)[N], const int lane) {
     const bool up = lane & K;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
@@ -236,13 +247,17 @@ __device__ __forceinline__ void butterfly_step(float (&v)[32], const int lane) {
     }
 }
 
-// After the call lane L holds in v[0] the sum over all lanes of v[L].
-__device__ __forceinline__ void transpose_reduce(float (&v)[32], const int lane) {
-    butterfly_step<16>(v, lane);
+// After the call lane L holds in v[0] the sum over all lanes of v[L % N]
+// (N = 32 or 16).
+template <int N>
+__device__ __forceinline__ void transpose_reduce(float (&v)[N], const int lane) {
+    static_assert(N == 32 || N == 16, "32 or 16 values per lane");
+    if (N == 32) butterfly_step<16>(v, lane);
     butterfly_step<8>(v, lane);
     butterfly_step<4>(v, lane);
     butterfly_step<2>(v, lane);
     butterfly_step<1>(v, lane);
+    if (N == 16) v[0] += __shfl_xor_sync(kFull, v[0], 16);
 }
 
 template <int SOFT, bool MASSES, int NC>
@@ -280,9 +295,10 @@ pair_split_src_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
         if (lane == 0) item = atomicAdd(a.queue, 1);
         item = __shfl_sync(kFull, item, 0);
         if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        const int li = item_leaf(a, item, lane);
+        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
         if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
+        const LeafMeta mt = a.leaf[li];
         for (int s0 = 0; s0 < mt.npart; s0 += 32) {
             const int ns = min(32, mt.npart - s0);
             // sinks of this slice in their own leaf frame; slots past ns repeat
@@ -382,6 +398,12 @@ struct SinkPair {
 #ifndef P2P_X2_MINBLOCKS
 #define P2P_X2_MINBLOCKS 3  // resident 128-thread blocks per SM the register budget targets
 #endif
+#ifndef P2P_X2_HOIST_COEF
+#define P2P_X2_HOIST_COEF 0  // packed coefficient pairs held in registers for the whole kernel
+#endif
+#ifndef P2P_X2_SINKPAIRS
+#define P2P_X2_SINKPAIRS 16  // sink pairs per slice (a slice holds 2x that many sinks)
+#endif
 constexpr int kPairGroup = P2P_X2_GROUP;
 
 // H(t) for two sinks at once. Horner: one packed FMA per coefficient.
@@ -390,7 +412,7 @@ constexpr int kPairGroup = P2P_X2_GROUP;
 // powers t^2, t^4, t^8 in packed FMAs; the dependency depth drops from NC-1
 // to about log2(NC) + 1.
 template <int NC>
-__device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
+__device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a, const float2 *cv) {
 #if P2P_X2_SCALAR_POLY
     // two scalar Horner chains: coefficients stay constant-bank operands
     float hx = a.coef[NC - 1], hy = a.coef[NC - 1];
@@ -425,6 +447,11 @@ __device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
         }
     }
     return q[0];
+#elif P2P_X2_HOIST_COEF
+    float2 h = cv[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, cv[k]);
+    return h;
 #else
     float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);
 #pragma unroll
@@ -440,7 +467,7 @@ template <int SOFT, bool MASSES, int NC, bool CHECK>
 __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
                                               const float sw, const SinkPair &p,
                                               const PairArgs &a, const float2 eps2v,
-                                              const float2 negu0v, float2 &ax, float2 &ay,
+                                              const float2 negu0v, const float2 *cv, float2 &ax, float2 &ay,
                                               float2 &az, bool &amb) {
     const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
     const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
@@ -455,7 +482,7 @@ __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, 
     }
     const float2 r = make_float2(rsqrt_approx(u.x), rsqrt_approx(u.y));
     const float2 t = __fadd2_rn(u, negu0v);
-    const float2 h = poly_x2<NC>(t, a);  // -H(u)
+    const float2 h = poly_x2<NC>(t, a, cv);  // -H(u)
     float2 f = __ffma2_rn(__fmul2_rn(r, r), r, h);
     if (CHECK) {
         const bool in_x = u.x <= a.ucut_lo, in_y = u.y <= a.ucut_lo;
@@ -505,24 +532,29 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
     extern __shared__ float4 smem_f4[];
     using Acc = typename AccSel<ACC>::T;
     const int lane = threadIdx.x & 31;
-    // per warp: 16 sink pairs (512 B), 32 band corrections (512 B), the
+    // per warp: up to 16 sink pairs (512 B), 32 band corrections (512 B), the
     // staged sources and their particle indices
+    constexpr int NP = P2P_X2_SINKPAIRS, NS = 2 * NP;
     float4 *region = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 64 + stage_cap / 4);
     SinkPair *sinks = reinterpret_cast<SinkPair *>(region);
     float4 *corr = region + 32;
     float4 *stage = region + 64;
     int *sidx = reinterpret_cast<int *>(stage + stage_cap);
     const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
+    float2 cv[NC];  // packed coefficient pairs (used when P2P_X2_HOIST_COEF)
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cv[k] = make_float2(a.coef[k], a.coef[k]);
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1);
         item = __shfl_sync(kFull, item, 0);
         if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        const int li = item_leaf(a, item, lane);
+        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
         if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
-        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
-            const int ns = min(32, mt.npart - s0);
+        const LeafMeta mt = a.leaf[li];
+        for (int s0 = 0; s0 < mt.npart; s0 += NS) {
+            const int ns = min(NS, mt.npart - s0);
             {
                 // slots past ns repeat the first sink so padded lanes stay finite
                 const float4 q = a.pos4[mt.ipart + s0 + (lane < ns ? lane : 0)];
@@ -534,15 +566,15 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                 corr[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             // packed partials: element .x of pair k is sink 2k, .y sink 2k+1
-            float2 ax[16], ay[16], az[16];
+            float2 ax[NP], ay[NP], az[NP];
 #pragma unroll
-            for (int i = 0; i < 16; ++i) ax[i] = ay[i] = az[i] = make_float2(0.f, 0.f);
+            for (int i = 0; i < NP; ++i) ax[i] = ay[i] = az[i] = make_float2(0.f, 0.f);
             Acc acc;
             int fill = 0, chunks = 0;
             auto flush = [&]() {
-                float vx[32], vy[32], vz[32];
+                float vx[NS], vy[NS], vz[NS];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
+                for (int i = 0; i < NP; ++i) {
                     vx[2 * i] = ax[i].x; vx[2 * i + 1] = ax[i].y;
                     vy[2 * i] = ay[i].x; vy[2 * i + 1] = ay[i].y;
                     vz[2 * i] = az[i].x; vz[2 * i + 1] = az[i].y;
@@ -552,7 +584,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                 transpose_reduce(vz, lane);
                 acc.add(vx[0], vy[0], vz[0]);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) ax[i] = ay[i] = az[i] = make_float2(0.f, 0.f);
+                for (int i = 0; i < NP; ++i) ax[i] = ay[i] = az[i] = make_float2(0.f, 0.f);
                 chunks = 0;
             };
             auto consume = [&]() {
@@ -570,22 +602,22 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                     bool amb = false;
                     if (check) {
 #pragma unroll
-                        for (int g = 0; g < 16; g += kPairGroup) {
+                        for (int g = 0; g < NP; g += kPairGroup) {
                             if (2 * g < ns) {
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
                                     pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                          negu0v, ax[g + q], ay[g + q], az[g + q], amb);
+                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     } else {
 #pragma unroll
-                        for (int g = 0; g < 16; g += kPairGroup) {
+                        for (int g = 0; g < NP; g += kPairGroup) {
                             if (2 * g < ns) {
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
                                     pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                           negu0v, ax[g + q], ay[g + q], az[g + q], amb);
+                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     }
@@ -715,9 +747,10 @@ pair_plain_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
         if (lane == 0) item = atomicAdd(a.queue, 1);
         item = __shfl_sync(kFull, item, 0);
         if (item >= a.nleaf) break;
-        const int64_t rb = a.row_off[item], re = a.row_off[item + 1];
+        const int li = item_leaf(a, item, lane);
+        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
         if (rb >= re) continue;
-        const LeafMeta mt = a.leaf[item];
+        const LeafMeta mt = a.leaf[li];
         for (int s0 = 0; s0 < mt.npart; s0 += 32) {
             const int ns = min(32, mt.npart - s0);
             const int gs = group_size(ns);

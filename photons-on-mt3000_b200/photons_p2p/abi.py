@@ -46,6 +46,36 @@ class Params(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("slots", ctypes.c_int),
+        ("max_pack", ctypes.c_int),
+        ("full_grid", ctypes.c_int),
+        ("hbm_bytes", ctypes.c_size_t),
+        ("rows_per_particle", ctypes.c_double),
+        ("particles_per_leaf", ctypes.c_double),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("requests_done", ctypes.c_int64),
+        ("launches", ctypes.c_int64),
+        ("boxes_launched", ctypes.c_int64),
+        ("builds", ctypes.c_int64),
+        ("evictions", ctypes.c_int64),
+        ("pairs", ctypes.c_int64),
+        ("kernel_ms", ctypes.c_double),
+        ("build_ms", ctypes.c_double),
+        ("resident_boxes", ctypes.c_int),
+        ("resident_bytes", ctypes.c_size_t),
+        ("capacity_bytes", ctypes.c_size_t),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _i64 = ctypes.c_int64
@@ -80,6 +110,21 @@ SIGNATURES = {
     "p2p_session_last_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     "p2p_measure_fp32_peak": (_i, [_vp, ctypes.POINTER(_d)]),
     "p2p_pass_noalloc": (_i, [ctypes.POINTER(Params), _i, _vp, _i, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
+    "p2p_server_config_default": (None, [ctypes.POINTER(ServerConfig)]),
+    "p2p_server_create": (_i, [_i, ctypes.POINTER(Params), ctypes.POINTER(ServerConfig),
+                               ctypes.POINTER(_vp)]),
+    "p2p_server_destroy": (_i, [_vp]),
+    "p2p_server_add_box": (_i, [_vp, _d, _d, _i, _vp, _i, _vp, _vp, _i64, _vp, _vp, _i, _vp,
+                                ctypes.POINTER(_i)]),
+    "p2p_server_preload": (_i, [_vp, _i]),
+    "p2p_server_box_bytes": (_i, [_vp, _i, ctypes.POINTER(ctypes.c_size_t)]),
+    "p2p_server_submit": (_i, [_vp, _i, _vp, ctypes.POINTER(_i64)]),
+    "p2p_server_wait": (_i, [_vp, _i64, ctypes.POINTER(_d)]),
+    "p2p_server_query": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_d)]),
+    "p2p_server_drain": (_i, [_vp]),
+    "p2p_server_get_stats": (_i, [_vp, ctypes.POINTER(ServerStats)]),
+    "p2p_host_alloc": (_i, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "p2p_host_free": (_i, [_vp]),
 }
 
 

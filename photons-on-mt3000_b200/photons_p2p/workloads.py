@@ -186,30 +186,35 @@ class ServingBox:
     cfg: PassConfig
 
 
+def c4_box(b, seed_offset=0, n_range=(32, 128)):
+    """Box b of the serving ensemble (independent periodic unit box, its own
+    seed): n^3 lattice points, n log-uniform in n_range, Gaussian displacement
+    sigma ~ U[0.1, 0.4] spacing, plus 0-200 NFW halos (c ~ U[4, 12], counts
+    from dN/dM ~ M^-1.9 on [100, 20000], total capped at n^3 / 2)."""
+    g = np.random.Generator(np.random.PCG64([MASTER_SEED + 4, seed_offset, b]))
+    n = int(round(np.exp(g.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+    sigma = g.uniform(0.1, 0.4)
+    pos = lattice_gaussian(n, sigma, g)
+    nh = int(g.integers(0, 201))
+    if nh:
+        cap = n ** 3 // 2
+        lo, hi, a = 100.0, 20000.0, -0.9
+        m = (lo ** a + g.random(nh) * (hi ** a - lo ** a)) ** (1.0 / a)
+        cnt = np.maximum(1, np.round(m)).astype(np.int64)
+        if cnt.sum() > cap:
+            cnt = np.maximum(1, np.floor(cnt * (cap / cnt.sum()))).astype(np.int64)
+        centres = g.random((nh, 3))
+        concs = g.uniform(4.0, 12.0, nh)
+        ntot = n ** 3 + int(cnt.sum())
+        extra = [nfw_halo(int(cnt[k]), cnt[k] / ntot, concs[k], centres[k], g) for k in range(nh)]
+        pos = np.mod(np.concatenate([pos] + extra, axis=1), 1.0)
+    cfg = PassConfig(f"c4_box{b}_{n}^3", n, n, 1.2, 4.5, SOFT_PLUMMER, 1.0 / (40 * n), 2.25, 32, 0.0)
+    return ServingBox(b, n, pos, cfg)
+
+
 def c4_boxes(nbox=512, seed_offset=0, n_range=(32, 128)):
-    """Serving ensemble: independent periodic unit boxes."""
-    g = rng(4 + seed_offset)
-    boxes = []
-    for b in range(nbox):
-        n = int(round(np.exp(g.uniform(np.log(n_range[0]), np.log(n_range[1])))))
-        sigma = g.uniform(0.1, 0.4)
-        pos = lattice_gaussian(n, sigma, g)
-        nh = int(g.integers(0, 201))
-        if nh:
-            cap = n ** 3 // 2
-            lo, hi, a = 100.0, 20000.0, -0.9
-            m = (lo ** a + g.random(nh) * (hi ** a - lo ** a)) ** (1.0 / a)
-            cnt = np.maximum(1, np.round(m)).astype(np.int64)
-            if cnt.sum() > cap:
-                cnt = np.maximum(1, np.floor(cnt * (cap / cnt.sum()))).astype(np.int64)
-            centres = g.random((nh, 3))
-            concs = g.uniform(4.0, 12.0, nh)
-            ntot = n ** 3 + int(cnt.sum())
-            extra = [nfw_halo(int(cnt[k]), cnt[k] / ntot, concs[k], centres[k], g) for k in range(nh)]
-            pos = np.mod(np.concatenate([pos] + extra, axis=1), 1.0)
-        cfg = PassConfig(f"c4_box{b}_{n}^3", n, n, 1.2, 4.5, SOFT_PLUMMER, 1.0 / (40 * n), 2.25, 32, 0.0)
-        boxes.append(ServingBox(b, n, pos, cfg))
-    return boxes
+    """Serving ensemble: independent periodic unit boxes (c4_box 0..nbox-1)."""
+    return [c4_box(b, seed_offset, n_range) for b in range(nbox)]
 
 
 def with_ghosts(pos, cfg):
