@@ -1,7 +1,7 @@
 """Benchmark of the B200 P2P short-range force pass.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload c2|c1|c2_128] [--form split|plain]
+                [--workload c2|c1|c2_128|c4] [--form split|plain]
 
 A step is one force pass over the workload's interaction lists. The default
 workload is the 256^3 clustered configuration (60% uniform, 40% in 2,000 NFW
@@ -13,10 +13,18 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
            resident in HBM, the whole pass (frame prep, CSR build, pair
            kernel) replayed as a CUDA graph, device time from CUDA events,
            L2 flushed between steps (inputs are also larger than L2)
+  accuracy the chosen form's per-particle force error against the plain
+           FP64 form on the same inputs (rms and max of |da| / |a|)
   e2e      the same metric through the C ABI on pinned host buffers:
            H2D of positions, leaves and lists, the pass, D2H of the forces
   roofline FP32 pipe: pairs/s x flops-per-pair (counted from the kernel
            source, FMA = 2) / the FP32 FFMA peak measured in-process
+  serving  48 boxes of the serving ensemble resident in one server:
+           saturation throughput, then Poisson arrivals at half of it,
+           p50 / p99 request latency (submit to result in host memory)
+
+--workload c4 runs the serving configuration alone: 512 boxes, Poisson
+arrivals at 0.25, 0.5, 1, 2 and 4 times the measured saturation rate.
 
 With --gpus N > 1 (torchrun, one rank per GPU) every rank runs its own
 independent box (replicas, no collective on the data path); the timed
@@ -26,6 +34,7 @@ FP32 SPI, compiled for the host from the reference sources into
 oracle/_ref) on the host cores, over a bounded sample of the same lists.
 """
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -40,7 +49,7 @@ sys.path[:0] = [REPO, os.path.join(REPO, "photons-on-mt3000_b200")]
 
 from photons_p2p import abi, workloads as W  # noqa: E402
 
-METRIC = "pair-interactions/s"
+METRIC = "pair-interactions/s at rms force err\u22641e-5 vs plain; ensemble p50/p99 latency"
 
 
 def flops_per_pair(soft_mode, degree, masses=False):
@@ -130,6 +139,20 @@ def load_traffic(workload, form_name):
         return None
 
 
+def combine_ranks(total_s, e2e_s, pairs, dist, device):
+    """Whole-job figures of a replica run: the slowest rank's times (max over
+    ranks) and the pair interactions of all ranks (sum)."""
+    if not dist:
+        return float(total_s), float(e2e_s), float(pairs)
+    import torch
+
+    t = torch.tensor([total_s, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    pt = torch.tensor([float(pairs)], dtype=torch.float64, device=device)
+    dist.all_reduce(pt, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(pt[0])
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -179,6 +202,12 @@ def run_ours(args, rank, world, dist):
             dist.barrier()
         return pass_s, kern_ms, launches
 
+    def result(sess):
+        out = np.empty((3, tl.npart))
+        if sess.lib.p2p_pass_result(sess.h, out.ctypes.data_as(ctypes.c_void_p)):
+            raise RuntimeError(sess.lib.p2p_last_error().decode())
+        return out
+
     with Session(local) as sess:
         fp32_peak = sess.measure_fp32_peak()
         sess.set_params(params_for(cfg, form, mass))
@@ -186,12 +215,21 @@ def run_ours(args, rank, world, dist):
         sampler = ClockSampler(local)
         pass_s, kern_ms, launches = resident_passes(sess, args.steps, args.warmup, sampler)
         clocks = sampler.summary()
-        # the plain FP64 form on the same inputs, for the split/plain ratio
-        plain = None
+        acc_form = result(sess)
+        # the plain FP64 form on the same inputs: the split/plain ratio and the
+        # chosen form's force error against it (local particles)
+        plain, accuracy = None, None
         if form == abi.FORM_SPLIT and not args.skip_plain:
             sess.set_params(params_for(cfg, abi.FORM_PLAIN_FP64, mass))
             p_s, p_k, _ = resident_passes(sess, max(1, min(args.steps, 3)), 1)
             plain = {"value": P / float(np.mean(p_s)), "kernel_ms": float(np.mean(p_k))}
+            loc = tl.tag == 1
+            acc_plain = result(sess)
+            num = np.linalg.norm(acc_form - acc_plain, axis=0)[loc]
+            den = np.linalg.norm(acc_plain, axis=0)[loc]
+            rel = num / np.where(den > 0, den, 1.0)
+            accuracy = {"vs": "plain_fp64", "rms": float(np.sqrt(np.mean(rel ** 2))),
+                        "max": float(rel.max()), "particles": int(loc.sum())}
             sess.set_params(params_for(cfg, form, mass))
 
         # e2e through the C ABI on pinned host buffers
@@ -200,7 +238,6 @@ def run_ours(args, rank, world, dist):
                                        pin(tl.task_t), pin(tl.task_s))
         h_out = torch.zeros((3, tl.npart), dtype=torch.float64).pin_memory()
         lib = sess.lib
-        import ctypes
 
         def e2e_pass():
             ok = lib.p2p_pass_begin(sess.h, tl.npart, h_pos.data_ptr(), None, tl.nleaf,
@@ -225,17 +262,7 @@ def run_ours(args, rank, world, dist):
     mean_kernel_ms = float(np.mean(kern_ms))
     total_s = float(np.sum(pass_s))
     e2e_mean = float(np.mean(e2e_t))
-    if dist:
-        import torch.distributed as tdist
-
-        t = torch.tensor([total_s, e2e_mean], dtype=torch.float64, device=dev)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        total_s, e2e_mean = float(t[0]), float(t[1])
-        pt = torch.tensor([float(P)], dtype=torch.float64, device=dev)
-        tdist.all_reduce(pt, op=tdist.ReduceOp.SUM)
-        P_all = float(pt[0])
-    else:
-        P_all = float(P)
+    total_s, e2e_mean, P_all = combine_ranks(total_s, e2e_mean, P, dist, dev)
     value = P_all * args.steps / total_s
     F = flops_per_pair(cfg.soft_mode, degree) if form != abi.FORM_PLAIN_FP64 else None
     kernel_pairs_per_s = P / (mean_kernel_ms * 1e-3)
@@ -264,12 +291,226 @@ def run_ours(args, rank, world, dist):
         "roofline": roofline,
         "plain_fp64": plain,
         "split_over_plain": (value / plain["value"]) if plain else None,
+        "accuracy": accuracy,
         "e2e": {"value": P_all / e2e_mean, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
     return out, cfg, tl, nlocal
+
+
+C4_EPS_OVER_RS = (1.0 / 40) / 1.2  # serving boxes: eps = 1/(40 n), r_s = 1.2 / n
+
+
+def serving_ensemble(srv, nbox, log=None):
+    """Registers and preloads serving boxes 0..nbox-1 (their host lists are
+    dropped once resident); returns (particles, pair interactions) totals."""
+    from photons_p2p import serve
+
+    npart = pairs = 0
+    for b in range(nbox):
+        box = W.c4_box(b)
+        tl = serve.box_lists(box)
+        k = srv.add_box(tl, 0.5 / box.cfg.split_radius, 1.0 / int(tl.tag.sum()))
+        srv.preload(k)
+        npart += tl.npart
+        pairs += srv.boxes[k].pairs
+        if log and (b + 1) % 64 == 0:
+            log(f"[serving] {b + 1}/{nbox} boxes resident")
+    return npart, pairs
+
+
+def serving_measure(srv, rates_frac, requests, seed=10):
+    """Saturation throughput (a burst of 2 requests per box), then Poisson
+    arrivals at the given fractions of it."""
+    from photons_p2p import serve
+
+    nbox = len(srv.boxes)
+    sat = serve.run_poisson(srv, 1e9, 2 * nbox, seed=seed, reserve=2)
+    rows = []
+    for i, f in enumerate(rates_frac):
+        rate = f * sat["requests_per_s"]
+        n = requests(rate) if callable(requests) else requests
+        r = serve.run_poisson(srv, rate, int(n), seed=seed + 1 + i)
+        r["rate_frac"] = f
+        rows.append(r)
+    return sat, rows
+
+
+def run_serving_leg(local, nbox=48):
+    """The serving summary of the default run: nbox ensemble boxes, one full
+    grid slot, Poisson arrivals at half the measured saturation rate."""
+    from photons_p2p import serve
+
+    t0 = time.time()
+    shape = serve.serving_shape(abi.FORM_SPLIT, C4_EPS_OVER_RS)
+    with serve.Server(shape, device=local, slots=1, full_grid=True, hbm_bytes=40 << 30) as srv:
+        npart, pairs = serving_ensemble(srv, nbox)
+        prep = time.time() - t0
+        sat, rows = serving_measure(srv, [0.5], 4 * nbox)
+    r = rows[0]
+    return {"boxes": nbox, "particles": int(npart), "slots": 1, "max_pack": 32,
+            "saturation_pairs_per_s": sat["pairs_per_s"],
+            "saturation_requests_per_s": sat["requests_per_s"],
+            "rate_hz": r["rate_hz"], "rate_frac_of_saturation": 0.5, "requests": r["requests"],
+            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "requests_per_s": r["requests_per_s"],
+            "pairs_per_s": r["pairs_per_s"], "boxes_per_launch": r["boxes_per_launch"],
+            "host_prep_s": round(prep, 1)}
+
+
+def run_serving_sweep(args, local):
+    """Serving configuration: 512 boxes (n^3, n log-uniform in [32, 128],
+    lattice + Gaussian + 0-200 NFW halos), Poisson arrivals at 0.25, 0.5, 1,
+    2 and 4 times the measured saturation throughput."""
+    from photons_p2p import serve
+
+    t0 = time.time()
+    shape = serve.serving_shape(abi.FORM_SPLIT, C4_EPS_OVER_RS)
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    with serve.Server(shape, device=local, slots=args.slots, full_grid=True,
+                      hbm_bytes=int(args.hbm_gb * (1 << 30))) as srv:
+        npart, pairs = serving_ensemble(srv, args.boxes, log)
+        prep = time.time() - t0
+        st0 = srv.stats()
+        sampler = ClockSampler(local)
+        with sampler:
+            sat, rows = serving_measure(srv, [0.25, 0.5, 1.0, 2.0, 4.0],
+                                        lambda rate: min(3000, max(200, rate * 6.0)))
+        st1 = srv.stats()
+    for r in rows:
+        log(f"[serving] {r['rate_frac']:.2f}x sat ({r['rate_hz']:.0f}/s): p50 {r['p50_ms']:.2f} ms "
+            f"p99 {r['p99_ms']:.2f} ms  {r['requests_per_s']:.1f} req/s  {r['pairs_per_s']:.3e} pairs/s")
+    sweep = [{k: r[k] for k in ("rate_frac", "rate_hz", "requests", "p50_ms", "p99_ms", "mean_ms",
+                                "max_ms", "requests_per_s", "pairs_per_s", "boxes_per_launch",
+                                "launches")} for r in rows]
+    out = {
+        "metric": METRIC, "value": sat["pairs_per_s"], "unit": "pairs/s", "n_gpus": 1,
+        "steps": len(rows), "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 leaf offsets + f64 accumulation)",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": f"c4_serving_{args.boxes}_boxes", "boxes": args.boxes,
+                   "particles_with_ghosts": int(npart), "pairs_per_round": int(pairs),
+                   "slots": args.slots, "max_pack": 32, "hbm_budget_gb": args.hbm_gb,
+                   "resident_gb": st1["resident_bytes"] / 1e9, "host_prep_s": round(prep, 1),
+                   "l2": "inputs > L2 (boxes resident, 126 MB L2)"},
+        "serving": {"saturation_pairs_per_s": sat["pairs_per_s"],
+                    "saturation_requests_per_s": sat["requests_per_s"],
+                    "saturation_p50_ms": sat["p50_ms"], "saturation_p99_ms": sat["p99_ms"],
+                    "sweep": sweep, "launches": st1["launches"] - st0["launches"],
+                    "kernel_s": (st1["kernel_ms"] - st0["kernel_ms"]) / 1e3},
+        "gpu_launches": int(3 * (st1["launches"] - st0["launches"])),
+        "clocks": sampler.summary(),
+        "cpu_baseline": None,
+    }
+    return out
+
+
+def run_batching(args, local):
+    """Batching configuration: side^3 particles (512^3 = 134M by default) of
+    the uniform / NFW mix with 20,000 halos (scaled by volume below 512),
+    leaf cap swept; for each cap the walk runs in groups of sink leaves
+    (bounded host memory) straight into device-resident list chunks, the
+    autotuner picks the launch shape on a sample, and whole passes (frame
+    prep, per-chunk CSR build, persistent pair kernel) are timed with CUDA
+    events, inputs resident in HBM."""
+    import torch
+
+    from photons_p2p import autotune
+    from photons_p2p.lists import Tree
+    from photons_p2p.p2p import Session, _check
+
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(local)
+    side = args.side
+    t0 = time.time()
+    nh = max(1, int(round(20000 * (side / 512.0) ** 3)))
+    pos, _ = W.clustered(side ** 3, 0.4, nh, (4.0, 12.0), W.rng(3))
+    base = W.scaled(W.c3_config(32), n_side=side, mesh=side, eps=1.0 / (40 * side))
+    allpos, tag = W.with_ghosts(pos, base)
+    nlocal = pos.shape[1]
+    del pos
+    mass = 1.0 / nlocal
+    log(f"[batching] {side}^3: {allpos.shape[1]} particles with ghosts, {time.time() - t0:.1f} s")
+    records = []
+    caps = [int(c) for c in args.leaf_caps.split(",")]
+    cache = args.tune_cache
+    for cap in caps:
+        cfg = W.scaled(base, name=f"c3_batching_{side}^3_leaf{cap}", maxleaf=cap)
+        t1 = time.time()
+        with Tree(allpos, tag, cap, cfg.box) as tree:
+            nleaf = tree.nleaf
+            # rows per sink leaf from a 1/64 sample walk sets the group count
+            probe = np.zeros(nleaf, np.uint8)
+            probe[::64] = 1
+            tt, _ = tree.walk(cfg.cutoff_radius, cfg.open_angle, probe)
+            est = len(tt) * 64
+            groups = max(1, int(np.ceil(est / args.chunk_rows)))
+            bounds = np.linspace(0, nleaf, groups + 1).astype(np.int64)
+            chunks, pairs, rows = [], 0, 0
+            npl = tree.leaf_npart.astype(np.int64)
+            sample_lists = None
+            for g in range(groups):
+                m = np.zeros(nleaf, np.uint8)
+                m[bounds[g]:bounds[g + 1]] = 1
+                tt, ts = tree.walk(cfg.cutoff_radius, cfg.open_angle, m)
+                if not len(tt):
+                    continue
+                pairs += int(np.dot(npl[tt], npl[ts]))
+                rows += len(tt)
+                if sample_lists is None:
+                    sample_lists = tree.lists(tt, ts)
+                chunks.append((torch.from_numpy(tt).to(dev), torch.from_numpy(ts).to(dev)))
+                del tt, ts
+            lists_s = time.time() - t1
+            d_pos = torch.from_numpy(tree.pos).to(dev)
+            d_ip = torch.from_numpy(tree.leaf_ipart).to(dev)
+            d_np = torch.from_numpy(tree.leaf_npart).to(dev)
+            npart = tree.pos.shape[1]
+            qs = np.percentile(tree.leaf_npart, [0, 25, 50, 75, 100]).tolist()
+            mean_leaf = float(tree.leaf_npart.mean())
+        log(f"[batching] cap {cap}: {nleaf} leaves (mean {mean_leaf:.1f}), {rows:.3e} rows in "
+            f"{len(chunks)} chunks, {pairs:.3e} pairs, lists {lists_s:.1f} s")
+        params, rec = autotune.tune(cfg, sample_lists, abi.FORM_SPLIT, mass, device=local,
+                                    sample_pairs=args.tune_pairs, cache_path=cache, log=log)
+        del sample_lists
+        with Session(local, params) as sess:
+            lib = sess.lib
+
+            def one_pass():
+                _check(lib, lib.p2p_pass_begin_device(sess.h, npart, d_pos.data_ptr(), None, nleaf,
+                                                      d_ip.data_ptr(), d_np.data_ptr()))
+                for ct, cs in chunks:
+                    _check(lib, lib.p2p_pass_submit_device(sess.h, ct.numel(), ct.data_ptr(), cs.data_ptr()))
+                return sess.end()
+
+            for _ in range(args.warmup):
+                one_pass()
+            secs = [one_pass() for _ in range(args.steps)]
+        pass_s = float(np.mean(secs))
+        r = {"leaf_cap": cap, "leaves": int(nleaf), "leaf_npart_q0_25_50_75_100": qs,
+             "mean_leaf": mean_leaf, "rows": int(rows), "rows_per_sink_leaf": rows / max(1, nleaf),
+             "chunks": len(chunks), "pairs": int(pairs), "pass_s": pass_s, "pairs_per_s": pairs / pass_s,
+             "tuned": {k: rec[k] for k in ("key", "variant", "stage", "warps", "cached")},
+             "lists_host_s": round(lists_s, 1)}
+        log(f"[batching] cap {cap}: pass {pass_s:.3f} s  {pairs / pass_s:.3e} pairs/s  shape "
+            f"{rec['variant']}/{rec['stage']}/{rec['warps']}")
+        records.append(r)
+        del chunks, d_pos, d_ip, d_np
+        torch.cuda.empty_cache()
+    head = next((r for r in records if r["leaf_cap"] == 32), records[0])
+    return {
+        "metric": METRIC, "value": head["pairs_per_s"], "unit": "pairs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * head["pass_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 leaf offsets + f64 accumulation)", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": f"c3_batching_{side}^3", "n_local": int(nlocal),
+                   "n_with_ghosts": int(allpos.shape[1]), "halos": nh, "leaf_caps": caps,
+                   "value_leaf_cap": head["leaf_cap"], "chunk_rows": args.chunk_rows,
+                   "l2": "inputs > L2"},
+        "batching": records, "cpu_baseline": None,
+    }
 
 
 class _Null:
@@ -332,6 +573,15 @@ def main():
     ap.add_argument("--cpu-pairs", type=float, default=2e9)
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving summary")
+    ap.add_argument("--boxes", type=int, default=512, help="c4: ensemble size")
+    ap.add_argument("--slots", type=int, default=1, help="c4: server launch slots")
+    ap.add_argument("--hbm-gb", type=float, default=100.0, help="c4: server arena size")
+    ap.add_argument("--side", type=int, default=512, help="c3: particles per side")
+    ap.add_argument("--leaf-caps", default="16,32,64", help="c3: leaf caps to sweep")
+    ap.add_argument("--chunk-rows", type=float, default=1.0e9, help="c3: list entries per chunk")
+    ap.add_argument("--tune-pairs", type=float, default=2e9, help="c3: autotuner sample size")
+    ap.add_argument("--tune-cache", default=None, help="c3: autotuner cache (JSON)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: fewer than 3 warm-up steps requested", file=sys.stderr)
@@ -372,7 +622,25 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.workload == "c3":
+        if rank == 0:
+            print(json.dumps(run_batching(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "c4":
+        if rank == 0:
+            print(json.dumps(run_serving_sweep(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     out, cfg, tl, nlocal = run_ours(args, rank, world, dist)
+    if world == 1 and not args.no_serving and args.workload == "c2":
+        out["serving"] = run_serving_leg(int(os.environ.get("LOCAL_RANK", "0")))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, _ = time_cpu(cfg, tl, 1.0 / nlocal, args.cpu_pairs)
         out["cpu_baseline"] = cb

@@ -21,6 +21,7 @@
 
 #include "photons_p2p.h"
 #include "p2p_fit.h"
+#include "p2p_args.h"
 #include "p2p_internal.h"
 
 // This file's own instance of the pass kernels: the header is compiled into
@@ -260,24 +261,7 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     a.queue = queue;
     a.npart = npart;
     a.nleaf = nleaf;
-    a.cscale = c;
-    a.eps2 = (float)((c * p.soften) * (c * p.soften));
-    a.u0 = (float)fit.u0;
-    a.ucut = (float)fit.umax;
-    a.ucut_lo = (float)(fit.umax * (1.0 - kCutBand));
-    a.ucut_hi = (float)(fit.umax * (1.0 + kCutBand));
-    a.rcut2 = fit.umax / (c * c);
-    a.eps2_box = p.soften * p.soften;
-    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = -fit.coef[k];
-    a.uin = (float)(fit.umax * (1.0 - kInsideMargin));
-    a.out_scale = c * c * p.mass;
-    a.soft = p.soften;
-    a.r_soft = 1.0 / p.soften;
-    a.rrs = 1.0 / p.split_radius;
-    a.hrrs = 0.5 * a.rrs;
-    a.coeff = 2.0 * (1.0 / std::sqrt(M_PI));
-    a.xcut = p.x_cut;
-    a.mass_eq = p.mass;
+    fill_pass_scalars(a, p, fit, false);
     if (fp32) {
         st = p.soft_mode == P2P_SOFT_CLAMP
                  ? launch_split<SOFT_CLAMP>(fit.ncoef_kernel, sms, warps, smem, s, a, stage)

@@ -401,6 +401,9 @@ struct SinkPair {
 #ifndef P2P_X2_HOIST_COEF
 #define P2P_X2_HOIST_COEF 0  // packed coefficient pairs held in registers for the whole kernel
 #endif
+#ifndef P2P_X2_COEF_PAIRS
+#define P2P_X2_COEF_PAIRS 0  // packed coefficient pairs from the parameters (no duplication per use)
+#endif
 #ifndef P2P_X2_SINKPAIRS
 #define P2P_X2_SINKPAIRS 16  // sink pairs per slice (a slice holds 2x that many sinks)
 #endif
@@ -451,6 +454,12 @@ __device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a, con
     float2 h = cv[NC - 1];
 #pragma unroll
     for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, cv[k]);
+    return h;
+#elif P2P_X2_COEF_PAIRS
+    // packed coefficient pairs read from the kernel parameters
+    float2 h = a.coef2[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, a.coef2[k]);
     return h;
 #else
     float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);

@@ -1,0 +1,131 @@
+"""Launch-shape autotuner of the pair kernel, keyed on the leaf-size histogram.
+
+The shape of a pass is (lane mapping, sources staged per warp, warps per
+block): the lane mapping fixes the sink tile (SINK_LANES: one sink per lane,
+rows of <= 16 sinks split their sources over 2-4 lanes; SOURCE_LANES: one
+staged source per lane against the row's <= 32 sinks; SOURCE_LANES_X2: the
+same with two sinks per packed f32x2 instruction), stage_sources is the
+source chunk a warp stages in shared memory before it computes, and every
+sink leaf is one warp's work item (the persistent kernel's work-stealing
+unit). Which shape wins depends on how many particles the leaves hold and
+how long the rows are, so tuned shapes are cached under a key built from the
+leaf-size histogram (quartiles of particles per leaf, mean list entries per
+sink leaf, leaf cap) plus the form and softening.
+
+tune() times every candidate on a sample of the pass (the rows of every
+k-th sink leaf, about `sample_pairs` pair interactions) with CUDA events and
+keeps the fastest.
+"""
+import json
+import os
+
+import numpy as np
+
+from . import abi
+from .p2p import Session, params_for
+
+CANDIDATES = [
+    (abi.VARIANT_SOURCE_LANES_X2, st, w) for st in (128, 256, 512, 1024) for w in (2, 4)
+] + [
+    (abi.VARIANT_SOURCE_LANES, st, w) for st in (256, 512) for w in (2, 4)
+] + [
+    (abi.VARIANT_SINK_LANES, st, w) for st in (128, 256) for w in (4, 8)
+]
+
+
+def histogram_key(leaf_npart, task_t, form, soft_mode):
+    """Cache key of a pass from its leaf-size histogram."""
+    n = np.asarray(leaf_npart)
+    active = np.unique(np.asarray(task_t))
+    q = np.percentile(n[active], [25, 50, 75]).round().astype(int) if active.size else [0, 0, 0]
+    rows = len(task_t) / max(1, active.size)
+    rows_bin = int(2 ** round(np.log2(max(rows, 1.0))))   # rows per sink leaf, to a power of 2
+    return (f"cap{int(n.max()) if n.size else 0}_q{q[0]}-{q[1]}-{q[2]}_rows{rows_bin}"
+            f"_{abi.FORM_NAMES[form]}_soft{soft_mode}")
+
+
+def sample_rows(leaf_npart, task_t, task_s, sample_pairs):
+    """The rows of every k-th sink leaf, k chosen so the sample holds about
+    sample_pairs pair interactions (the whole list if it is smaller)."""
+    n = np.asarray(leaf_npart, np.int64)
+    tt, ts = np.asarray(task_t), np.asarray(task_s)
+    total = float(np.dot(n[tt], n[ts]))
+    k = max(1, int(total // max(sample_pairs, 1.0)))
+    if k == 1:
+        return tt, ts, int(total)
+    keep = (tt % k) == 0
+    st, ss = tt[keep], ts[keep]
+    return st, ss, int(np.dot(n[st], n[ss]))
+
+
+def load_cache(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def save_cache(path, cache):
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(cache, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, repeats=2,
+         candidates=CANDIDATES, log=None):
+    """Best launch shape for this pass; returns (params, record). With
+    cache_path, a cached record under the same key is reused and new results
+    are stored."""
+    import torch
+
+    key = histogram_key(lists.leaf_npart, lists.task_t, form, cfg.soft_mode)
+    cache = load_cache(cache_path) if cache_path else {}
+    base = params_for(cfg, form, mass)
+
+    def apply(rec):
+        p = params_for(cfg, form, mass)
+        p.kernel_variant, p.stage_sources, p.warps_per_block = rec["variant"], rec["stage"], rec["warps"]
+        return p
+
+    if key in cache:
+        return apply(cache[key]), dict(cache[key], key=key, cached=True)
+    st, ss, pairs = sample_rows(lists.leaf_npart, lists.task_t, lists.task_s, sample_pairs)
+    dev = torch.device("cuda", device)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (lists.pos, lists.leaf_ipart, lists.leaf_npart, st, ss)]
+    args = (lists.npart, d[0].data_ptr(), lists.nleaf, d[1].data_ptr(), d[2].data_ptr(), len(st),
+            d[3].data_ptr(), d[4].data_ptr())
+    results = []
+    cands = candidates if form != abi.FORM_PLAIN_FP64 else [(0, st_, w) for st_ in (64, 128, 256)
+                                                              for w in (2, 4, 8)]
+    with Session(device) as s:
+        for variant, stage, warps in cands:
+            p = params_for(cfg, form, mass)
+            p.kernel_variant, p.stage_sources, p.warps_per_block = variant, stage, warps
+            try:
+                s.set_params(p)
+                ms = []
+                for _ in range(repeats + 1):
+                    s.run_device(*args)
+                    s.end()
+                    ms.append(s.last_kernel_ms())
+            except Exception as e:  # a shape that does not fit is skipped
+                if log:
+                    log(f"[tune] {variant}/{stage}/{warps}: {e}")
+                continue
+            t = min(ms[1:])
+            results.append({"variant": variant, "stage": stage, "warps": warps, "kernel_ms": t,
+                            "pairs_per_s": pairs / (t * 1e-3)})
+            if log:
+                log(f"[tune] variant {variant} stage {stage} warps {warps}: {t:.3f} ms "
+                    f"{pairs / (t * 1e-3):.3e} pairs/s")
+    best = max(results, key=lambda r: r["pairs_per_s"])
+    rec = dict(best, sample_pairs=pairs, candidates=len(results))
+    if cache_path:
+        cache = load_cache(cache_path)
+        cache[key] = rec
+        save_cache(cache_path, cache)
+    del base
+    return apply(rec), dict(rec, key=key, cached=False, all=results)

@@ -75,42 +75,81 @@ class TreeLists:
         return int(np.dot(n[self.task_t], n[self.task_s]))
 
 
+class Tree:
+    """A kd-tree (src/fmm.c:231-327) kept for several walks, e.g. the walk of
+    one group of sink leaves at a time when the whole list would not fit in
+    host memory. pos (3, n) float64, tag (n,) int: 1 local, 0 ghost."""
+
+    def __init__(self, pos, tag, maxleaf, boxsize):
+        self.lib = _native.lists()
+        self.pos = np.array(pos, dtype=np.float64, order="C", copy=True)
+        tag = np.ascontiguousarray(tag, dtype=np.int32)
+        n = self.pos.shape[1]
+        self.perm = np.empty(n, dtype=np.int32)
+        self.h = self.lib.p2p_tree_build(n, _ptr(self.pos, _f64p), _ptr(tag, _i32p), maxleaf, boxsize,
+                                         _ptr(self.perm, _i32p))
+        if not self.h:
+            raise RuntimeError("tree build failed")
+        self.tag = tag[self.perm]
+        nleaf = self.lib.p2p_tree_nleaf(self.h)
+        self.leaf_ipart = np.empty(nleaf, np.int32)
+        self.leaf_npart = np.empty(nleaf, np.int32)
+        self.leaf_active = np.empty(nleaf, np.int32)
+        self.leaf_center = np.empty((nleaf, 3), np.float64)
+        self.leaf_width = np.empty((nleaf, 3), np.float64)
+        self.lib.p2p_tree_leaves(self.h, _ptr(self.leaf_ipart, _i32p), _ptr(self.leaf_npart, _i32p),
+                                 _ptr(self.leaf_active, _i32p), _ptr(self.leaf_center, _f64p),
+                                 _ptr(self.leaf_width, _f64p))
+
+    @property
+    def nleaf(self):
+        return self.leaf_npart.shape[0]
+
+    def walk(self, cutoff, open_angle, leaf_mask=None):
+        """(task_t, task_s) of the P2P walk (src/fmm.c:656-792); with
+        leaf_mask (nleaf bools) only the rows of the masked sink leaves, in
+        the full walk's order."""
+        if leaf_mask is None:
+            nt = self.lib.p2p_tree_walk(self.h, cutoff, open_angle)
+        else:
+            m = np.ascontiguousarray(leaf_mask, dtype=np.uint8)
+            nt = self.lib.p2p_tree_walk_masked(self.h, cutoff, open_angle, m.ctypes.data_as(ctypes.c_void_p))
+        tt = np.empty(nt, np.int32)
+        ts = np.empty(nt, np.int32)
+        self.lib.p2p_tree_tasks(self.h, _ptr(tt, _i32p), _ptr(ts, _i32p))
+        return tt, ts
+
+    def lists(self, task_t, task_s):
+        return TreeLists(pos=self.pos, perm=self.perm, tag=self.tag, leaf_ipart=self.leaf_ipart,
+                         leaf_npart=self.leaf_npart, leaf_active=self.leaf_active,
+                         leaf_center=self.leaf_center, leaf_width=self.leaf_width, task_t=task_t,
+                         task_s=task_s)
+
+    def close(self):
+        if self.h:
+            self.lib.p2p_tree_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def build_tree_lists(pos, tag, maxleaf, boxsize, cutoff, open_angle, sink_particles=None):
     """kd-tree (src/fmm.c:231-327) + P2P walk (src/fmm.c:656-792) over the
     given particles (pos (3, n) float64, tag (n,) int: 1 local, 0 ghost).
     sink_particles (original indices, optional) keeps only the list rows of
     the leaves holding them (the same entries, in the same order)."""
-    lib = _native.lists()
-    pos = np.array(pos, dtype=np.float64, order="C", copy=True)
-    tag = np.ascontiguousarray(tag, dtype=np.int32)
-    n = pos.shape[1]
-    perm = np.empty(n, dtype=np.int32)
-    h = lib.p2p_tree_build(n, _ptr(pos, _f64p), _ptr(tag, _i32p), maxleaf, boxsize,
-                           _ptr(perm, _i32p))
-    if not h:
-        raise RuntimeError("tree build failed")
-    try:
-        nleaf = lib.p2p_tree_nleaf(h)
-        ip = np.empty(nleaf, np.int32)
-        npt = np.empty(nleaf, np.int32)
-        act = np.empty(nleaf, np.int32)
-        ctr = np.empty((nleaf, 3), np.float64)
-        wid = np.empty((nleaf, 3), np.float64)
-        lib.p2p_tree_leaves(h, _ptr(ip, _i32p), _ptr(npt, _i32p), _ptr(act, _i32p),
-                            _ptr(ctr, _f64p), _ptr(wid, _f64p))
-        if sink_particles is None:
-            nt = lib.p2p_tree_walk(h, cutoff, open_angle)
-        else:
+    with Tree(pos, tag, maxleaf, boxsize) as t:
+        mask = None
+        if sink_particles is not None:
+            n = t.pos.shape[1]
             slot = np.empty(n, np.int64)
-            slot[perm] = np.arange(n)
-            leaf_of_slot = np.repeat(np.arange(nleaf), npt)
-            mask = np.zeros(nleaf, np.uint8)
+            slot[t.perm] = np.arange(n)
+            leaf_of_slot = np.repeat(np.arange(t.nleaf), t.leaf_npart)
+            mask = np.zeros(t.nleaf, np.uint8)
             mask[leaf_of_slot[slot[np.asarray(sink_particles)]]] = 1
-            nt = lib.p2p_tree_walk_masked(h, cutoff, open_angle, mask.ctypes.data_as(ctypes.c_void_p))
-        tt = np.empty(nt, np.int32)
-        ts = np.empty(nt, np.int32)
-        lib.p2p_tree_tasks(h, _ptr(tt, _i32p), _ptr(ts, _i32p))
-    finally:
-        lib.p2p_tree_free(h)
-    return TreeLists(pos=pos, perm=perm, tag=tag[perm], leaf_ipart=ip, leaf_npart=npt,
-                     leaf_active=act, leaf_center=ctr, leaf_width=wid, task_t=tt, task_s=ts)
+        tt, ts = t.walk(cutoff, open_angle, mask)
+        return t.lists(tt, ts)
