@@ -77,7 +77,12 @@ typedef struct {
 #define P2P_VARIANT_AUTO 0            /* the fastest mapping (P2P_VARIANT_SOURCE_LANES_X2) */
 #define P2P_VARIANT_SINK_LANES 1      /* one lane per sink particle, sources broadcast */
 #define P2P_VARIANT_SOURCE_LANES 2    /* one lane per staged source, sinks broadcast */
-#define P2P_VARIANT_SOURCE_LANES_X2 3 /* source lanes, two sinks per packed f32x2 instruction */
+#define P2P_VARIANT_SOURCE_LANES_X2 3 /* source lanes, two sinks per packed f32x2 instruction,
+                                         32-sink tile */
+#define P2P_VARIANT_SOURCE_LANES_X2_S16 4 /* the same with a 16-sink tile (fewer registers,
+                                             more resident warps; for small leaves) */
+#define P2P_VARIANT_SINK_LANES_X2 5       /* packed sink lanes: each lane keeps a sink pair,
+                                             the leaf's pairs share the lanes' sources */
 
 typedef struct p2p_session p2p_session;
 

@@ -144,7 +144,7 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 1024]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
-    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SOURCE_LANES_X2)
+    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SINK_LANES_X2)
         return fail(P2P_ERR_ARG, "unknown kernel_variant %d", p->kernel_variant);
     if (p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES &&
         p->warps_per_block > 4)
@@ -153,7 +153,8 @@ int validate_params(const p2p_params *p) {
         const int w = p->warps_per_block ? p->warps_per_block : 4;
         const int st = p->stage_sources ? p->stage_sources : (p->form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
         const size_t smem = p->form == P2P_FORM_PLAIN_FP64 ? pair_smem_plain(w, st)
-                            : std::max(pair_smem_x2(w, st), pair_smem_split(w, st, true));
+                            : std::max(std::max(pair_smem_x2(w, st), pair_smem_sx2(w, st)),
+                                       pair_smem_split(w, st, true));
         if (smem > (size_t)227 * 1024)
             return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
     }
@@ -171,7 +172,8 @@ bool source_lanes(const p2p_params &p) {
 
 bool packed_lanes(const p2p_params &p) {
     return p.form != P2P_FORM_PLAIN_FP64 &&
-           (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2);
+           (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2 ||
+            p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16);
 }
 
 int default_stage(const p2p_params &p) {
@@ -193,9 +195,12 @@ int launch_pair(p2p_session *s, const PairArgs &a) {
     L.blocks_per_sm = p.blocks_per_sm;
     L.dry_run = s->dry_run;
     L.occ = &s->occupancy;
+    L.sink_pairs = p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16 ? 8 : 16;
     PairLaunchResult r;
     if (p.form == P2P_FORM_PLAIN_FP64)
         r = launch_pair_plain(L, a);
+    else if (p.kernel_variant == P2P_VARIANT_SINK_LANES_X2)
+        r = launch_pair_sink_lanes_x2(L, a);
     else if (packed_lanes(p))
         r = launch_pair_source_lanes_x2(L, a);
     else if (source_lanes(p))
@@ -214,6 +219,7 @@ cudaError_t allow_smem_all() {
     cudaError_t e = allow_smem_sink_lanes();
     if (e == cudaSuccess) e = allow_smem_source_lanes();
     if (e == cudaSuccess) e = allow_smem_source_lanes_x2();
+    if (e == cudaSuccess) e = allow_smem_sink_lanes_x2();
     if (e == cudaSuccess) e = allow_smem_plain();
     return e;
 }

@@ -27,6 +27,7 @@ struct PairLaunch {
     bool dry_run;       // resolve the launch shape only
     OccupancyCache *occ;
     int max_blocks = 0; // > 0: cap on the persistent grid (a share of the GPU)
+    int sink_pairs = 16; // packed source-lane kernel: sink pairs per slice (16 or 8)
 };
 
 struct PairLaunchResult {
@@ -42,6 +43,8 @@ inline size_t pair_smem_split(int warps, int stage, bool source_lanes) {
 inline size_t pair_smem_plain(int warps, int stage) { return (size_t)warps * stage * 32; }
 // packed source-lane kernel: sink pairs, band corrections, staged sources + their indices
 inline size_t pair_smem_x2(int warps, int stage) { return (size_t)warps * (stage + 64 + stage / 4) * 16; }
+// packed sink-lane kernel: staged sources as two float4 + index, 32 padding slots
+inline size_t pair_smem_sx2(int warps, int stage) { return (size_t)warps * (stage + 32) * 36; }
 
 // Persistent grid for `kernel`: blocks_per_sm, or as many as registers and
 // shared memory let reside (queried once and cached).
@@ -83,6 +86,7 @@ PairLaunchResult launch_persistent(const PairLaunch &L, K kernel, size_t smem, c
 PairLaunchResult launch_pair_sink_lanes(const PairLaunch &L, const PairArgs &a);
 PairLaunchResult launch_pair_source_lanes(const PairLaunch &L, const PairArgs &a);
 PairLaunchResult launch_pair_source_lanes_x2(const PairLaunch &L, const PairArgs &a);
+PairLaunchResult launch_pair_sink_lanes_x2(const PairLaunch &L, const PairArgs &a);
 // FP64 form.
 PairLaunchResult launch_pair_plain(const PairLaunch &L, const PairArgs &a);
 
@@ -90,6 +94,7 @@ PairLaunchResult launch_pair_plain(const PairLaunch &L, const PairArgs &a);
 cudaError_t allow_smem_sink_lanes();
 cudaError_t allow_smem_source_lanes();
 cudaError_t allow_smem_source_lanes_x2();
+cudaError_t allow_smem_sink_lanes_x2();
 cudaError_t allow_smem_plain();
 
 }  // namespace p2p

@@ -2,6 +2,8 @@
 // mappings and the FP64 drop-in form.
 #pragma once
 
+#include <type_traits>
+
 #include "p2p_device_common.cuh"
 
 namespace p2p {
@@ -234,7 +236,10 @@ pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
 // component) so that lane i holds sink i's sum, which it adds to its FP64
 // (or Kahan / FP32) total.
 constexpr int kSinkGroup = 4;        // sinks evaluated per predicated block
-constexpr int kSrcFlushChunks = 32;  // FP32 partial depth per lane, in chunks
+#ifndef P2P_FLUSH_CHUNKS
+#define P2P_FLUSH_CHUNKS 32
+#endif
+constexpr int kSrcFlushChunks = P2P_FLUSH_CHUNKS;  // FP32 partial depth per lane, in chunks
 
 template <int K, int N>
 __device__ __forceinline__ void butterfly_step(float (&v)[N], const int lane) {
@@ -404,6 +409,12 @@ struct SinkPair {
 #ifndef P2P_X2_COEF_PAIRS
 #define P2P_X2_COEF_PAIRS 0  // packed coefficient pairs from the parameters (no duplication per use)
 #endif
+#ifndef P2P_X2_ALWAYS_CHECK
+#define P2P_X2_ALWAYS_CHECK 0  // one code path: every chunk takes the cutoff select and band test
+#endif
+#ifndef P2P_X2_TWO_SOURCES
+#define P2P_X2_TWO_SOURCES 0  // two staged sources per lane per step
+#endif
 #ifndef P2P_X2_SINKPAIRS
 #define P2P_X2_SINKPAIRS 16  // sink pairs per slice (a slice holds 2x that many sinks)
 #endif
@@ -535,15 +546,18 @@ __device__ __forceinline__ bool band_pair(const float4 src, const float psx, con
     return true;
 }
 
-template <int SOFT, bool MASSES, int ACC, int NC>
-__global__ void __launch_bounds__(128, P2P_X2_MINBLOCKS)
+// NP sink pairs per slice: 16 (32-sink tile, 3 blocks of 4 warps per SM) or
+// 8 (16-sink tile, half the partial registers, 4 blocks per SM).
+template <int SOFT, bool MASSES, int ACC, int NC, int NP = P2P_X2_SINKPAIRS>
+__global__ void __launch_bounds__(128, NP == 8 ? 4 : P2P_X2_MINBLOCKS)
 pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
     extern __shared__ float4 smem_f4[];
     using Acc = typename AccSel<ACC>::T;
     const int lane = threadIdx.x & 31;
     // per warp: up to 16 sink pairs (512 B), 32 band corrections (512 B), the
     // staged sources and their particle indices
-    constexpr int NP = P2P_X2_SINKPAIRS, NS = 2 * NP;
+    constexpr int NS = 2 * NP;
+    static_assert(NP == 8 || NP == 16, "8 or 16 sink pairs per slice");
     float4 *region = smem_f4 + (threadIdx.x >> 5) * (stage_cap + 64 + stage_cap / 4);
     SinkPair *sinks = reinterpret_cast<SinkPair *>(region);
     float4 *corr = region + 32;
@@ -599,6 +613,50 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
             auto consume = [&]() {
                 __syncwarp();
                 unsigned ambmask = 0;  // chunks of this batch with a pair in the cutoff band
+#if P2P_X2_TWO_SOURCES
+                // two staged sources per lane per step: twice the independent
+                // dependency chains for the same sink pairs
+                for (int c = 0, ci = 0; c < fill; c += 64, ci += 2) {
+                    const int slot0 = c + lane, slot1 = c + 32 + lane;
+                    const float4 far = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+                    const float4 s0 = slot0 < fill ? stage[slot0] : far;
+                    const float4 s1 = slot1 < fill ? stage[slot1] : far;
+                    const float2 sx0 = make_float2(s0.x, s0.x), sy0 = make_float2(s0.y, s0.y),
+                                 sz0 = make_float2(s0.z, s0.z);
+                    const float2 sx1 = make_float2(s1.x, s1.x), sy1 = make_float2(s1.y, s1.y),
+                                 sz1 = make_float2(s1.z, s1.z);
+                    const bool check = __any_sync(kFull, slot1 >= fill || sidx[slot0] < 0 || sidx[slot1] < 0);
+                    bool amb0 = false, amb1 = false;
+                    if (check) {
+#pragma unroll
+                        for (int g = 0; g < NP; g += kPairGroup) {
+                            if (2 * g < ns) {
+#pragma unroll
+                                for (int q = 0; q < kPairGroup; ++q) {
+                                    pair_split_x2<SOFT, MASSES, NC, true>(sx0, sy0, sz0, s0.w, sinks[g + q], a, eps2v,
+                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb0);
+                                    pair_split_x2<SOFT, MASSES, NC, true>(sx1, sy1, sz1, s1.w, sinks[g + q], a, eps2v,
+                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb1);
+                                }
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int g = 0; g < NP; g += kPairGroup) {
+                            if (2 * g < ns) {
+#pragma unroll
+                                for (int q = 0; q < kPairGroup; ++q) {
+                                    pair_split_x2<SOFT, MASSES, NC, false>(sx0, sy0, sz0, s0.w, sinks[g + q], a, eps2v,
+                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb0);
+                                    pair_split_x2<SOFT, MASSES, NC, false>(sx1, sy1, sz1, s1.w, sinks[g + q], a, eps2v,
+                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb1);
+                                }
+                            }
+                        }
+                    }
+                    ambmask |= (amb0 ? (1u << ci) : 0u) | (amb1 ? (2u << ci) : 0u);
+                }
+#else
                 for (int c = 0, ci = 0; c < fill; c += 32, ++ci) {
                     const int slot = c + lane;
                     const float4 src = slot < fill ? stage[slot]
@@ -607,7 +665,11 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                                  sz = make_float2(src.z, src.z);
                     // full chunks whose sources all come from entries inside the
                     // cutoff skip the select and the band test
+#if P2P_X2_ALWAYS_CHECK
+                    const bool check = true;
+#else
                     const bool check = __any_sync(kFull, slot >= fill || sidx[slot] < 0);
+#endif
                     bool amb = false;
                     if (check) {
 #pragma unroll
@@ -632,6 +694,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                     }
                     ambmask |= amb ? (1u << ci) : 0u;
                 }
+#endif
                 // rare: pairs within the cutoff band, decided in FP64
                 if (__any_sync(kFull, ambmask != 0u)) {
                     while (ambmask) {
@@ -709,6 +772,187 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                 a.acc[(size_t)a.npart + idx] += acc.vy() * a.out_scale;
                 a.acc[2 * (size_t)a.npart + idx] += acc.vz() * a.out_scale;
             }
+        }
+    }
+}
+
+// ------------------------------------------- pair: FP32, packed sink lanes ---
+
+// Packed sink-lane mapping (P2P_VARIANT_SINK_LANES_X2). A slice of <= 32
+// sinks is held as npairs = ceil(ns / 2) sink pairs; lane = (pair p, phase j)
+// with P = npairs lanes per phase and J = floor(32 / P) phases: lane (p, j)
+// keeps sink pair p in registers (one f32x2 per coordinate) and takes the
+// staged sources j, j + J, j + 2J, ... (sources are staged pre-duplicated,
+// (x, x, y, y) (z, z, w, w), so they load as packed operands). Per lane the
+// FP32 partials are one f32x2 per component, flushed into the two sinks'
+// accumulators every kSinkFlushIters sources; at row end the J phases of a
+// pair are summed with shuffles. A pair whose FP32 u falls in the cutoff band
+// is re-decided at once from FP64 positions (band_pair) by its own lane.
+constexpr int kSinkFlushIters = 128;
+
+template <int SOFT, bool MASSES, int ACC, int NC>
+__global__ void __launch_bounds__(128, 5)
+pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
+    extern __shared__ float4 smem_f4[];
+    using Acc = typename AccSel<ACC>::T;
+    const int lane = threadIdx.x & 31;
+    // per warp: staged sources (two float4 each) and their particle indices,
+    // with room for up to 32 padding slots past stage_cap
+    const int cap = stage_cap + 32;
+    float4 *stage = smem_f4 + (threadIdx.x >> 5) * (2 * cap + cap / 4);
+    int *sidx = reinterpret_cast<int *>(stage + 2 * cap);
+    const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
+    float2 cv[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) cv[k] = make_float2(a.coef[k], a.coef[k]);
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.queue, 1);
+        item = __shfl_sync(kFull, item, 0);
+        if (item >= a.nleaf) break;
+        const int li = item_leaf(a, item, lane);
+        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
+        if (rb >= re) continue;
+        const LeafMeta mt = a.leaf[li];
+        for (int s0 = 0; s0 < mt.npart; s0 += 32) {
+            const int ns = min(32, mt.npart - s0);
+            const int npairs = (ns + 1) >> 1;
+            const int P = npairs, J = 32 / npairs;
+            const int p = lane % P, j = lane / P;
+            const bool owner = j < J;  // lanes past P * J take no sources
+            // this lane's sink pair (a missing second sink repeats the first)
+            const int sa = 2 * p, sb = min(2 * p + 1, ns - 1);
+            const float4 qa = a.pos4[mt.ipart + s0 + sa], qb = a.pos4[mt.ipart + s0 + sb];
+            SinkPair sp;
+            sp.xy = make_float4(-qa.x, -qb.x, -qa.y, -qb.y);
+            sp.z = make_float2(-qa.z, -qb.z);
+            float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
+            Acc acc_a, acc_b;
+            int iters = 0;
+            auto consume = [&](int fill) {
+                // pad to whole iterations with far sources that take the
+                // cutoff test (they contribute nothing)
+                const int nit = (fill + J - 1) / J;
+                for (int q = fill + lane; q < nit * J; q += 32) {
+                    stage[2 * q] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 1.0e4f);
+                    stage[2 * q + 1] = make_float4(1.0e4f, 1.0e4f, 0.f, 0.f);
+                    sidx[q] = (int)0x80000000;
+                }
+                __syncwarp();
+                for (int it = 0; it < nit; ++it) {
+                    // lanes past P * J read slot 0 and their results are never used
+                    const int slot = owner ? it * J + j : 0;
+                    const float4 A = stage[2 * slot];
+                    const float4 B = stage[2 * slot + 1];
+                    const int sid = sidx[slot];
+                    const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w),
+                                 sz = make_float2(B.x, B.y);
+                    const bool check = __any_sync(kFull, owner && sid < 0);
+                    bool amb = false;
+                    if (check)
+                        pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay, az,
+                                                              amb);
+                    else
+                        pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
+                                                               az, amb);
+                    if (amb && owner) {
+                        // rare: a pair inside the cutoff band, decided in FP64
+                        const float4 src = make_float4(A.x, A.z, B.x, B.z);
+                        const int isrc = sid & 0x7fffffff;
+                        float3 cb;
+                        if (band_pair<SOFT, MASSES, NC>(src, sp.xy.x, sp.xy.z, sp.z.x, isrc, mt.ipart + s0 + sa, a,
+                                                        &cb)) {
+                            ax.x += cb.x;
+                            ay.x += cb.y;
+                            az.x += cb.z;
+                        }
+                        if (sb != sa &&
+                            band_pair<SOFT, MASSES, NC>(src, sp.xy.y, sp.xy.w, sp.z.y, isrc, mt.ipart + s0 + sb, a,
+                                                        &cb)) {
+                            ax.y += cb.x;
+                            ay.y += cb.y;
+                            az.y += cb.z;
+                        }
+                    }
+                    if (++iters == kSinkFlushIters) {
+                        acc_a.add(ax.x, ay.x, az.x);
+                        acc_b.add(ax.y, ay.y, az.y);
+                        ax = ay = az = make_float2(0.f, 0.f);
+                        iters = 0;
+                    }
+                }
+                __syncwarp();
+            };
+            int fill = 0;
+            for (int64_t e0 = rb; e0 < re; e0 += 32) {
+                const int ne = (int)min((int64_t)32, re - e0);
+                int sip = 0, snp = 0, chk = 0;
+                float ox = 0.f, oy = 0.f, oz = 0.f;
+                if (lane < ne) {
+                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+                    sip = ms.ipart;
+                    snp = ms.npart;
+                    ox = (float)((ms.cx - mt.cx) * a.cscale);
+                    oy = (float)((ms.cy - mt.cy) * a.cscale);
+                    oz = (float)((ms.cz - mt.cz) * a.cscale);
+                    const float bx = fabsf(ox) + ms.hx + mt.hx, by = fabsf(oy) + ms.hy + mt.hy,
+                                bz = fabsf(oz) + ms.hz + mt.hz;
+                    const float umax_entry = fmaf(bx, bx, fmaf(by, by, fmaf(bz, bz, a.eps2)));
+                    chk = umax_entry < a.uin ? 0 : (int)0x80000000;
+                }
+                for (int jj = 0; jj < ne; ++jj) {
+                    const int jnp = __shfl_sync(kFull, snp, jj);
+                    const int jip = __shfl_sync(kFull, sip, jj);
+                    const int jchk = __shfl_sync(kFull, chk, jj);
+                    const float jx = __shfl_sync(kFull, ox, jj);
+                    const float jy = __shfl_sync(kFull, oy, jj);
+                    const float jz = __shfl_sync(kFull, oz, jj);
+                    int q0 = 0;
+                    while (q0 < jnp) {
+                        if (fill == stage_cap) {
+                            consume(fill);
+                            fill = 0;
+                        }
+                        const int take = min(jnp - q0, stage_cap - fill);
+                        for (int q = lane; q < take; q += 32) {
+                            const float4 v = a.pos4[jip + q0 + q];
+                            const float x = v.x + jx, y = v.y + jy, z = v.z + jz;
+                            stage[2 * (fill + q)] = make_float4(x, x, y, y);
+                            stage[2 * (fill + q) + 1] = make_float4(z, z, v.w, v.w);
+                            sidx[fill + q] = (jip + q0 + q) | jchk;
+                        }
+                        fill += take;
+                        q0 += take;
+                    }
+                }
+            }
+            if (fill) consume(fill);
+            acc_a.add(ax.x, ay.x, az.x);
+            acc_b.add(ax.y, ay.y, az.y);
+            // sum the J phases of each sink pair into phase 0
+            double t[6] = {acc_a.vx(), acc_a.vy(), acc_a.vz(), acc_b.vx(), acc_b.vy(), acc_b.vz()};
+            for (int ph = 1; ph < J; ++ph) {
+                const int from = (lane + ph * P) & 31;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const double v = __shfl_sync(kFull, t[k], from);
+                    if (j == 0) t[k] += v;
+                }
+            }
+            if (j == 0 && p < npairs) {
+                const size_t n = (size_t)a.npart;
+                const int ia = mt.ipart + s0 + sa;
+                a.acc[ia] += t[0] * a.out_scale;
+                a.acc[n + ia] += t[1] * a.out_scale;
+                a.acc[2 * n + ia] += t[2] * a.out_scale;
+                if (2 * p + 1 < ns) {
+                    const int ib = mt.ipart + s0 + 2 * p + 1;
+                    a.acc[ib] += t[3] * a.out_scale;
+                    a.acc[n + ib] += t[4] * a.out_scale;
+                    a.acc[2 * n + ib] += t[5] * a.out_scale;
+                }
+            }
+            __syncwarp();  // the stage is rewritten by the next slice
         }
     }
 }

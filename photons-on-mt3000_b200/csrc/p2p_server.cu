@@ -511,6 +511,7 @@ void CUDART_CB on_copy_done(void *p) {
 PairLaunchResult dispatch_pair(const p2p_params &p, const PairLaunch &L, const PairArgs &a) {
     if (p.form == P2P_FORM_PLAIN_FP64) return launch_pair_plain(L, a);
     if (p.kernel_variant == P2P_VARIANT_SINK_LANES) return launch_pair_sink_lanes(L, a);
+    if (p.kernel_variant == P2P_VARIANT_SINK_LANES_X2) return launch_pair_sink_lanes_x2(L, a);
     if (p.kernel_variant == P2P_VARIANT_SOURCE_LANES) return launch_pair_source_lanes(L, a);
     return launch_pair_source_lanes_x2(L, a);
 }
@@ -578,6 +579,7 @@ int launch_pack(p2p_server *S, Slot &sl, const std::vector<Job> &jobs) {
     L.dry_run = false;
     L.occ = &S->occ;
     L.max_blocks = 0;
+    L.sink_pairs = p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16 ? 8 : 16;
     if (!S->cfg.full_grid && S->cfg.slots > 1) {
         // a share of the resident blocks (the occupancy query runs once, dry)
         PairLaunch D = L;

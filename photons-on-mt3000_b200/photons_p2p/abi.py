@@ -21,6 +21,8 @@ VARIANT_AUTO = 0
 VARIANT_SINK_LANES = 1
 VARIANT_SOURCE_LANES = 2
 VARIANT_SOURCE_LANES_X2 = 3
+VARIANT_SOURCE_LANES_X2_S16 = 4
+VARIANT_SINK_LANES_X2 = 5
 
 FORM_NAMES = {
     FORM_PLAIN_FP64: "plain_fp64",

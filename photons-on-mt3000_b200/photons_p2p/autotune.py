@@ -1,16 +1,17 @@
 """Launch-shape autotuner of the pair kernel, keyed on the leaf-size histogram.
 
-The shape of a pass is (lane mapping, sources staged per warp, warps per
-block): the lane mapping fixes the sink tile (SINK_LANES: one sink per lane,
-rows of <= 16 sinks split their sources over 2-4 lanes; SOURCE_LANES: one
-staged source per lane against the row's <= 32 sinks; SOURCE_LANES_X2: the
-same with two sinks per packed f32x2 instruction), stage_sources is the
-source chunk a warp stages in shared memory before it computes, and every
-sink leaf is one warp's work item (the persistent kernel's work-stealing
-unit). Which shape wins depends on how many particles the leaves hold and
-how long the rows are, so tuned shapes are cached under a key built from the
-leaf-size histogram (quartiles of particles per leaf, mean list entries per
-sink leaf, leaf cap) plus the form and softening.
+The shape of a pass is (mapping and sink tile, sources staged per warp,
+warps per block): the packed source-lane kernel holds a slice of a sink leaf
+in registers against one staged source per lane (32 sinks, SOURCE_LANES_X2,
+or 16 sinks with half the partial registers and more resident warps,
+SOURCE_LANES_X2_S16); the packed sink-lane kernel keeps one sink pair per
+lane and spreads the staged sources over the lanes (SINK_LANES_X2),
+stage_sources is the source chunk a warp stages in shared memory before it
+computes, and every sink leaf is one warp's work item (the persistent
+kernel's work-stealing unit). Which shape wins depends on how many particles
+the leaves hold and how long the rows are, so tuned shapes are cached under
+a key built from the leaf-size histogram (quartiles of particles per leaf,
+mean list entries per sink leaf, leaf cap) plus the form and softening.
 
 tune() times every candidate on a sample of the pass (the rows of every
 k-th sink leaf, about `sample_pairs` pair interactions) with CUDA events and
@@ -24,13 +25,14 @@ import numpy as np
 from . import abi
 from .p2p import Session, params_for
 
+# Shapes of the packed kernels, the mappings that re-decide pairs in the
+# cutoff band from FP64 positions (the scalar sink-lane and source-lane
+# mappings keep an FP32 cutoff decision and are not candidates for the
+# FP32/FP64-split form's accuracy bar).
 CANDIDATES = [
-    (abi.VARIANT_SOURCE_LANES_X2, st, w) for st in (128, 256, 512, 1024) for w in (2, 4)
-] + [
-    (abi.VARIANT_SOURCE_LANES, st, w) for st in (256, 512) for w in (2, 4)
-] + [
-    (abi.VARIANT_SINK_LANES, st, w) for st in (128, 256) for w in (4, 8)
-]
+    (v, st, w) for v in (abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SOURCE_LANES_X2_S16)
+    for st in (128, 256, 512) for w in (2, 4)
+] + [(abi.VARIANT_SINK_LANES_X2, st, w) for st in (128, 256, 512) for w in (2, 4)]
 
 
 def histogram_key(leaf_npart, task_t, form, soft_mode):
@@ -82,7 +84,6 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, re
 
     key = histogram_key(lists.leaf_npart, lists.task_t, form, cfg.soft_mode)
     cache = load_cache(cache_path) if cache_path else {}
-    base = params_for(cfg, form, mass)
 
     def apply(rec):
         p = params_for(cfg, form, mass)
@@ -127,5 +128,4 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, re
         cache = load_cache(cache_path)
         cache[key] = rec
         save_cache(cache_path, cache)
-    del base
     return apply(rec), dict(rec, key=key, cached=False, all=results)

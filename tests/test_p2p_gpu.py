@@ -73,7 +73,8 @@ def test_plain_matches_oracle_c1_plummer(gpu, c1):
     assert mx <= PLAIN_MAX, (rms, mx)
 
 
-VARIANTS = [abi.VARIANT_SINK_LANES, abi.VARIANT_SOURCE_LANES, abi.VARIANT_SOURCE_LANES_X2]
+VARIANTS = [abi.VARIANT_SINK_LANES, abi.VARIANT_SOURCE_LANES, abi.VARIANT_SOURCE_LANES_X2,
+            abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
