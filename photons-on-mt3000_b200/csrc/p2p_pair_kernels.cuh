@@ -546,6 +546,78 @@ __device__ __forceinline__ bool band_pair(const float4 src, const float psx, con
     return true;
 }
 
+#ifndef P2P_FLAT_STAGE
+#define P2P_FLAT_STAGE 1  // stage a row's sources with all lanes' loads in flight at once
+#endif
+
+// Stages the sources of row entries [rb, re) of sink leaf mt: each source
+// leaf's FP32 coordinates shifted into the sink's frame by the FP32-rounded
+// FP64 offset of the two frames, with its particle index and, in the sign
+// bit, whether its entry can reach the cutoff band (box bound on u >= uin).
+// Sources of up to 32 entries are numbered consecutively (a warp prefix sum
+// of their sizes) and every lane takes every 32nd of them, finding its entry
+// by a binary search over the prefix sums, so a whole stage's global loads
+// are in flight together. store(slot, source, index) writes one staged
+// source; consume() empties the stage (fill = 0) when it is full.
+template <class Store, class Consume>
+__device__ __forceinline__ void stage_row_flat(const PairArgs &a, const LeafMeta &mt, const int64_t rb,
+                                               const int64_t re, const int lane, const int stage_cap,
+                                               int &fill, Store &&store, Consume &&consume) {
+    for (int64_t e0 = rb; e0 < re; e0 += 32) {
+        const int ne = (int)min((int64_t)32, re - e0);
+        int sip = 0, snp = 0, chk = 0;
+        float ox = 0.f, oy = 0.f, oz = 0.f;
+        if (lane < ne) {
+            const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
+            sip = ms.ipart;
+            snp = ms.npart;
+            ox = (float)((ms.cx - mt.cx) * a.cscale);
+            oy = (float)((ms.cy - mt.cy) * a.cscale);
+            oz = (float)((ms.cz - mt.cz) * a.cscale);
+            // largest u any pair of this entry can reach (box bound)
+            const float bx = fabsf(ox) + ms.hx + mt.hx, by = fabsf(oy) + ms.hy + mt.hy,
+                        bz = fabsf(oz) + ms.hz + mt.hz;
+            const float umax_entry = fmaf(bx, bx, fmaf(by, by, fmaf(bz, bz, a.eps2)));
+            chk = umax_entry < a.uin ? 0 : (int)0x80000000;
+        }
+        int incl = snp;  // inclusive prefix sum of the entries' sizes
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(kFull, incl, 31);
+        int done = 0;
+        while (done < total) {
+            if (fill == stage_cap) consume();
+            const int take = min(total - done, stage_cap - fill);
+            for (int t0 = 0; t0 < take; t0 += 32) {
+                const int t = t0 + lane;
+                const int g = done + min(t, take - 1);  // this lane's source (idle lanes repeat the last)
+                // its entry: the first one whose inclusive prefix exceeds g
+                int e = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int probe = __shfl_sync(kFull, incl, e + step - 1);
+                    if (probe <= g) e += step;
+                }
+                const int q = g - (__shfl_sync(kFull, incl, e) - __shfl_sync(kFull, snp, e));
+                const int jip = __shfl_sync(kFull, sip, e);
+                const int jchk = __shfl_sync(kFull, chk, e);
+                const float jx = __shfl_sync(kFull, ox, e);
+                const float jy = __shfl_sync(kFull, oy, e);
+                const float jz = __shfl_sync(kFull, oz, e);
+                if (t < take) {
+                    const float4 v = a.pos4[jip + q];
+                    store(fill + t, make_float4(v.x + jx, v.y + jy, v.z + jz, v.w), (jip + q) | jchk);
+                }
+            }
+            fill += take;
+            done += take;
+        }
+    }
+}
+
 // NP sink pairs per slice: 16 (32-sink tile, 3 blocks of 4 warps per SM) or
 // 8 (16-sink tile, half the partial registers, 4 blocks per SM).
 template <int SOFT, bool MASSES, int ACC, int NC, int NP = P2P_X2_SINKPAIRS>
@@ -723,6 +795,14 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                 fill = 0;
                 if (chunks >= kSrcFlushChunks) flush();
             };
+#if P2P_FLAT_STAGE
+            stage_row_flat(a, mt, rb, re, lane, stage_cap, fill,
+                           [&](int slot, const float4 v, int idx) {
+                               stage[slot] = v;
+                               sidx[slot] = idx;
+                           },
+                           consume);
+#else
             for (int64_t e0 = rb; e0 < re; e0 += 32) {
                 const int ne = (int)min((int64_t)32, re - e0);
                 int sip = 0, snp = 0, chk = 0;
@@ -761,6 +841,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                     }
                 }
             }
+#endif
             if (fill) consume();
             if (chunks) flush();
             __syncwarp();  // sinks[] and corr[] are rewritten by the next slice
@@ -839,42 +920,57 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                     sidx[q] = (int)0x80000000;
                 }
                 __syncwarp();
-                for (int it = 0; it < nit; ++it) {
-                    // lanes past P * J read slot 0 and their results are never used
-                    const int slot = owner ? it * J + j : 0;
-                    const float4 A = stage[2 * slot];
-                    const float4 B = stage[2 * slot + 1];
-                    const int sid = sidx[slot];
-                    const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w),
-                                 sz = make_float2(B.x, B.y);
-                    const bool check = __any_sync(kFull, owner && sid < 0);
-                    bool amb = false;
-                    if (check)
-                        pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay, az,
-                                                              amb);
-                    else
-                        pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
-                                                               az, amb);
-                    if (amb && owner) {
-                        // rare: a pair inside the cutoff band, decided in FP64
-                        const float4 src = make_float4(A.x, A.z, B.x, B.z);
-                        const int isrc = sid & 0x7fffffff;
-                        float3 cb;
-                        if (band_pair<SOFT, MASSES, NC>(src, sp.xy.x, sp.xy.z, sp.z.x, isrc, mt.ipart + s0 + sa, a,
-                                                        &cb)) {
-                            ax.x += cb.x;
-                            ay.x += cb.y;
-                            az.x += cb.z;
-                        }
-                        if (sb != sa &&
-                            band_pair<SOFT, MASSES, NC>(src, sp.xy.y, sp.xy.w, sp.z.y, isrc, mt.ipart + s0 + sb, a,
-                                                        &cb)) {
-                            ax.y += cb.x;
-                            ay.y += cb.y;
-                            az.y += cb.z;
+                // lanes past P * J stay on slot 0; their results are never used
+                const float4 *pa = stage + 2 * (owner ? j : 0);
+                const int *ps = sidx + (owner ? j : 0);
+                const int da = owner ? 2 * J : 0, ds = owner ? J : 0;
+                for (int ib = 0; ib < nit; ib += 32) {
+                    const int nb = min(32, nit - ib);
+                    unsigned ambbits = 0;  // iterations of this block with a pair in the cutoff band
+#pragma unroll 2
+                    for (int k = 0; k < nb; ++k) {
+                        const float4 A = pa[0];
+                        const float4 B = pa[1];
+                        const int sid = *ps;
+                        pa += da;
+                        ps += ds;
+                        const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w),
+                                     sz = make_float2(B.x, B.y);
+                        bool amb = false;
+                        if (__any_sync(kFull, owner && sid < 0))
+                            pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
+                                                                  az, amb);
+                        else
+                            pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
+                                                                   az, amb);
+                        ambbits |= amb ? (1u << k) : 0u;
+                    }
+                    // rare: pairs inside the cutoff band, decided in FP64 by the owning lane
+                    if (owner) {
+                        while (ambbits) {
+                            const int k = __ffs(ambbits) - 1;
+                            ambbits &= ambbits - 1;
+                            const int slot = (ib + k) * J + j;
+                            const float4 A = stage[2 * slot], B = stage[2 * slot + 1];
+                            const float4 src = make_float4(A.x, A.z, B.x, B.z);
+                            const int isrc = sidx[slot] & 0x7fffffff;
+                            float3 cb;
+                            if (band_pair<SOFT, MASSES, NC>(src, sp.xy.x, sp.xy.z, sp.z.x, isrc, mt.ipart + s0 + sa,
+                                                            a, &cb)) {
+                                ax.x += cb.x;
+                                ay.x += cb.y;
+                                az.x += cb.z;
+                            }
+                            if (sb != sa && band_pair<SOFT, MASSES, NC>(src, sp.xy.y, sp.xy.w, sp.z.y, isrc,
+                                                                        mt.ipart + s0 + sb, a, &cb)) {
+                                ax.y += cb.x;
+                                ay.y += cb.y;
+                                az.y += cb.z;
+                            }
                         }
                     }
-                    if (++iters == kSinkFlushIters) {
+                    iters += nb;
+                    if (iters >= kSinkFlushIters) {
                         acc_a.add(ax.x, ay.x, az.x);
                         acc_b.add(ax.y, ay.y, az.y);
                         ax = ay = az = make_float2(0.f, 0.f);
@@ -884,6 +980,18 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                 __syncwarp();
             };
             int fill = 0;
+#if P2P_FLAT_STAGE
+            stage_row_flat(a, mt, rb, re, lane, stage_cap, fill,
+                           [&](int slot, const float4 v, int idx) {
+                               stage[2 * slot] = make_float4(v.x, v.x, v.y, v.y);
+                               stage[2 * slot + 1] = make_float4(v.z, v.z, v.w, v.w);
+                               sidx[slot] = idx;
+                           },
+                           [&]() {
+                               consume(fill);
+                               fill = 0;
+                           });
+#else
             for (int64_t e0 = rb; e0 < re; e0 += 32) {
                 const int ne = (int)min((int64_t)32, re - e0);
                 int sip = 0, snp = 0, chk = 0;
@@ -926,6 +1034,7 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                     }
                 }
             }
+#endif
             if (fill) consume(fill);
             acc_a.add(ax.x, ay.x, az.x);
             acc_b.add(ax.y, ay.y, az.y);
