@@ -546,6 +546,10 @@ __device__ __forceinline__ bool band_pair(const float4 src, const float psx, con
     return true;
 }
 
+#ifndef P2P_STAGE_UNROLL
+#define P2P_STAGE_UNROLL 1  // rounds of 32 staged sources unrolled (loads of several rounds in flight)
+#endif
+constexpr int kStageUnroll = P2P_STAGE_UNROLL;
 #ifndef P2P_FLAT_STAGE
 #define P2P_FLAT_STAGE 1  // stage a row's sources with all lanes' loads in flight at once
 #endif
@@ -591,6 +595,7 @@ __device__ __forceinline__ void stage_row_flat(const PairArgs &a, const LeafMeta
         while (done < total) {
             if (fill == stage_cap) consume();
             const int take = min(total - done, stage_cap - fill);
+#pragma unroll kStageUnroll
             for (int t0 = 0; t0 < take; t0 += 32) {
                 const int t = t0 + lane;
                 const int g = done + min(t, take - 1);  // this lane's source (idle lanes repeat the last)
