@@ -73,6 +73,10 @@ struct p2p_session {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr, ev_k0 = nullptr, ev_k1 = nullptr;
+    // pipelined host submits: list pieces uploaded on copy_stream into two
+    // buffer pairs while the previous piece computes on stream
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t piece_ready[2] = {nullptr, nullptr}, piece_free[2] = {nullptr, nullptr};
     bool kernel_timed = false;
     bool dry_run = false;  // dispatch without launching (fills the occupancy cache)
     int last_blocks = 0;
@@ -80,8 +84,9 @@ struct p2p_session {
     p2p_params params{};
     PolyFit fit;
     // device buffers
+    DevBuf task_t2, task_s2;  // second buffer pair of pipelined submits
     DevBuf pos, mass, leaf_ip, leaf_np, task_t, task_s, meta, pos4, counts, fill, row_off,
-        row_src, tile_sums, acc, status, queue, pairs, probe;
+        row_src, tile_sums, acc, status, queue, pairs, skipped, probe;
     DevBuf keys_a, keys_b, vals_b, hist, hoffs, hsums;  // radix sort of the list
     // pass state
     bool in_pass = false;
@@ -124,6 +129,11 @@ int ensure(p2p_session *s, DevBuf &b, size_t bytes) {
 }
 
 bool is_fp32_form(int form) { return form != P2P_FORM_PLAIN_FP64; }
+
+// Host list submits longer than 2 * kPipePieceMin entries are uploaded and
+// computed in about kPipePieces pieces of at least kPipePieceMin entries.
+constexpr int64_t kPipePieceMin = (int64_t)1 << 25;
+constexpr int64_t kPipePieces = 8;
 
 int validate_params(const p2p_params *p) {
     if (p->form < P2P_FORM_PLAIN_FP64 || p->form > P2P_FORM_KAHAN_FP32)
@@ -288,7 +298,8 @@ int size_radix_buffers(p2p_session *s, int64_t ntask) {
 }
 
 // CSR build + pair kernel for one list chunk already on the device.
-int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed) {
+int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed,
+                  cudaEvent_t lists_read = nullptr) {
     if (ntask <= 0 || s->nleaf <= 0) return P2P_OK;
     CsrBufs b;
     b.counts = (int *)s->counts.p;
@@ -302,11 +313,19 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
     b.hoffs = (int64_t *)s->hoffs.p;
     b.hsums = (int64_t *)s->hsums.p;
     b.pairs = (unsigned long long *)s->pairs.p;
+    if (packed_lanes(s->params) ||
+        (is_fp32_form(s->params.form) && s->params.kernel_variant == P2P_VARIANT_SINK_LANES_X2)) {
+        // the packed kernels skip entries wholly beyond the cutoff; count their pairs
+        b.skipped = (unsigned long long *)s->skipped.p;
+        b.cscale = 0.5 / s->params.split_radius;
+        b.uout = (float)(s->fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin));
+    }
     b.status = (int *)s->status.p;
     int launched = 0;
     CUDA_TRY(enqueue_csr_build(s->stream, ntask, d_t, d_s, s->nleaf, (const LeafMeta *)s->meta.p, b,
                                &launched));
     launch_count(launched);
+    if (lists_read) CUDA_TRY(cudaEventRecord(lists_read, s->stream));  // d_t / d_s may be reused
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
     // Inside a stream capture the kernel's events become external event-record
@@ -339,6 +358,7 @@ int size_pass_buffers(p2p_session *s, int npart, int nleaf, bool host_inputs, bo
     P2P_TRY(ensure(s, s->status, sizeof(int)));
     P2P_TRY(ensure(s, s->queue, sizeof(int)));
     P2P_TRY(ensure(s, s->pairs, sizeof(unsigned long long)));
+    P2P_TRY(ensure(s, s->skipped, sizeof(unsigned long long)));
     return P2P_OK;
 }
 
@@ -346,6 +366,7 @@ int begin_common(p2p_session *s) {
     CUDA_TRY(cudaMemsetAsync(s->acc.p, 0, sizeof(double) * 3 * (size_t)s->npart, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
     CUDA_TRY(cudaMemsetAsync(s->pairs.p, 0, sizeof(unsigned long long), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->skipped.p, 0, sizeof(unsigned long long), s->stream));
     return enqueue_prep(s);
 }
 
@@ -427,6 +448,11 @@ P2P_API int p2p_session_create(int device, p2p_session **out) {
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_end);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_k0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_k1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        e = cudaEventCreateWithFlags(&s->piece_ready[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->piece_free[k], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = allow_smem_all();
     if (e != cudaSuccess) {
         delete s;
@@ -444,14 +470,18 @@ P2P_API int p2p_session_destroy(p2p_session *s) {
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     DevBuf *bufs[] = {&s->pos, &s->mass, &s->leaf_ip, &s->leaf_np, &s->task_t, &s->task_s,
                       &s->meta, &s->pos4, &s->counts, &s->fill, &s->row_off, &s->row_src,
-                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->probe,
-                      &s->keys_a, &s->keys_b, &s->vals_b, &s->hist, &s->hoffs, &s->hsums};
+                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->skipped, &s->probe,
+                      &s->keys_a, &s->keys_b, &s->vals_b, &s->hist, &s->hoffs, &s->hsums,
+                      &s->task_t2, &s->task_s2};
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
-    cudaEvent_t evs[] = {s->ev_begin, s->ev_end, s->ev_k0, s->ev_k1};
+    cudaEvent_t evs[] = {s->ev_begin, s->ev_end, s->ev_k0, s->ev_k1, s->piece_ready[0], s->piece_ready[1],
+                         s->piece_free[0], s->piece_free[1]};
     for (cudaEvent_t ev : evs)
         if (ev) cudaEventDestroy(ev);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     delete s;
     return P2P_OK;
 }
@@ -548,6 +578,36 @@ P2P_API int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, co
     if (ntask < 0) return fail(P2P_ERR_ARG, "negative ntask");
     if (ntask == 0) return P2P_OK;
     if (!task_t || !task_s) return fail(P2P_ERR_ARG, "null task list");
+    if (ntask > 2 * kPipePieceMin) {
+        // Large lists: upload in pieces on the copy stream while the previous
+        // piece's CSR build and pair kernel run (each piece is a list chunk,
+        // as the reference's LEN_TASK chunks are).
+        const int64_t piece = std::max<int64_t>(kPipePieceMin, (ntask + kPipePieces - 1) / kPipePieces);
+        P2P_TRY(ensure(s, s->task_t, sizeof(int) * (size_t)piece));
+        P2P_TRY(ensure(s, s->task_s, sizeof(int) * (size_t)piece));
+        P2P_TRY(ensure(s, s->task_t2, sizeof(int) * (size_t)piece));
+        P2P_TRY(ensure(s, s->task_s2, sizeof(int) * (size_t)piece));
+        P2P_TRY(size_radix_buffers(s, piece));
+        DevBuf *bt[2] = {&s->task_t, &s->task_t2}, *bs[2] = {&s->task_s, &s->task_s2};
+        // the copy stream starts after everything queued so far (begin's uploads)
+        CUDA_TRY(cudaEventRecord(s->piece_ready[0], s->stream));
+        CUDA_TRY(cudaStreamWaitEvent(s->copy_stream, s->piece_ready[0], 0));
+        bool used[2] = {false, false};
+        for (int64_t i0 = 0, k = 0; i0 < ntask; i0 += piece, k ^= 1) {
+            const int64_t n = std::min(piece, ntask - i0);
+            if (used[k]) CUDA_TRY(cudaStreamWaitEvent(s->copy_stream, s->piece_free[k], 0));
+            CUDA_TRY(cudaMemcpyAsync(bt[k]->p, task_t + i0, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                                     s->copy_stream));
+            CUDA_TRY(cudaMemcpyAsync(bs[k]->p, task_s + i0, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                                     s->copy_stream));
+            CUDA_TRY(cudaEventRecord(s->piece_ready[k], s->copy_stream));
+            CUDA_TRY(cudaStreamWaitEvent(s->stream, s->piece_ready[k], 0));
+            P2P_TRY(enqueue_chunk(s, n, (const int *)bt[k]->p, (const int *)bs[k]->p, i0 + n >= ntask,
+                                  s->piece_free[k]));
+            used[k] = true;
+        }
+        return P2P_OK;
+    }
     P2P_TRY(ensure(s, s->task_t, sizeof(int) * (size_t)ntask));
     P2P_TRY(ensure(s, s->task_s, sizeof(int) * (size_t)ntask));
     P2P_TRY(size_radix_buffers(s, ntask));
@@ -612,6 +672,17 @@ P2P_API int p2p_session_synchronize(p2p_session *s) {
 P2P_API int p2p_pass_result_device(p2p_session *s, const double **d_acc) {
     if (!s || !d_acc) return fail(P2P_ERR_ARG, "null argument");
     *d_acc = (const double *)s->acc.p;
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_evaluated_pairs(p2p_session *s, int64_t *pairs) {
+    P2P_TRY(check_session(s));
+    if (!pairs) return fail(P2P_ERR_ARG, "null argument");
+    unsigned long long v = 0, k = 0;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(cudaMemcpy(&v, s->pairs.p, sizeof(v), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&k, s->skipped.p, sizeof(k), cudaMemcpyDeviceToHost));
+    *pairs = (int64_t)(v - k);
     return P2P_OK;
 }
 

@@ -259,3 +259,53 @@ def test_run_device_graph_matches_host_path(gpu, dropin32):
             rms, mx = rel_err(out, host, tl.tag == 1)
             assert mx <= 1e-12, (rms, mx)
             assert s.pair_count() == tl.pair_count()
+
+
+@pytest.mark.parametrize("variant", [abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SINK_LANES_X2])
+def test_skipped_entries_change_nothing(gpu, c1, variant):
+    """The packed kernels skip list entries whose particles lie wholly beyond
+    the cutoff. The skipped pairs are counted (evaluated <= listed, and some
+    are skipped on this lattice), and the forces agree with the scalar
+    source-lane kernel, which evaluates every listed pair, to FP32 rounding."""
+    cfg, tl, mass, _ = c1
+    with Session(gpu) as s:
+        prm = params_for(cfg, abi.FORM_SPLIT, mass)
+        prm.kernel_variant = variant
+        s.set_params(prm)
+        got, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+        listed, evaluated = s.pair_count(), s.evaluated_pairs()
+        prm.kernel_variant = abi.VARIANT_SOURCE_LANES
+        s.set_params(prm)
+        ref, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+        assert s.evaluated_pairs() == s.pair_count() == listed == tl.pair_count()
+    assert 0 < evaluated < listed
+    # the scalar kernel decides cutoff-band pairs in FP32, so single particles
+    # may differ by up to the two forms' bounds together
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert rms <= 1e-6 and mx <= 2e-3
+
+
+def test_pipelined_host_submit_matches_resident_pass(gpu):
+    """A host list longer than 2^26 entries is uploaded in pieces on a copy
+    stream while earlier pieces compute; the result equals the resident
+    single-chunk pass up to the FP32 grouping of the pieces' partial sums."""
+    import torch
+
+    side = 128
+    cfg = W.scaled(W.c2_config(), n_side=side, mesh=side, eps=1 / (40 * side), maxleaf=16)
+    tl = W.prepare(W.c2_positions(side), cfg)
+    assert tl.ntask > 2 ** 26
+    mass = 1.0 / int(tl.tag.sum())
+    dev = torch.device("cuda", gpu)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+         for a in (tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)]
+    with Session(gpu, params_for(cfg, abi.FORM_SPLIT, mass)) as s:
+        got, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+        assert s.pair_count() == tl.pair_count()
+        s.run_device(tl.npart, d[0].data_ptr(), tl.nleaf, d[1].data_ptr(), d[2].data_ptr(), tl.ntask,
+                     d[3].data_ptr(), d[4].data_ptr())
+        s.end()
+        ref = np.zeros((3, tl.npart))
+        s.accumulate(ref)
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert rms <= 1e-6 and mx <= 1e-4, (rms, mx)
