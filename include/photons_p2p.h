@@ -136,6 +136,11 @@ int p2p_pass_result_device(p2p_session *s, const double **d_acc);
 /* Pair-interaction count sum(n_sink * n_source) of the chunks submitted in
  * the current pass, counted on the device (src/gpu_entry.cu:53-58). */
 int p2p_pass_pair_count(p2p_session *s, int64_t *pairs);
+/* No counterpart in the reference: of those, the pair interactions the
+ * kernels evaluated. The packed FP32 kernels skip list entries whose
+ * particles' bounding boxes lie wholly beyond the cutoff (all their pairs
+ * would be dropped, so the result is the same); the count excludes them. */
+int p2p_pass_evaluated_pairs(p2p_session *s, int64_t *pairs);
 
 /* Whole pass on device-resident inputs in one call, enqueued on the session
  * stream without waiting: zero, prepare, CSR build, pair kernel. The launch

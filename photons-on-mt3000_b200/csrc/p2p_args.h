@@ -33,6 +33,7 @@ inline void fill_pass_scalars(PairArgs &a, const p2p_params &p, const PolyFit &f
     a.eps2_2 = make_float2(a.eps2, a.eps2);
     a.negu0_2 = make_float2(-a.u0, -a.u0);
     a.uin = (float)(fit.umax * (1.0 - kInsideMargin));
+    a.uout = (float)(fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin));
     a.out_scale = c * c * (per_particle_masses ? 1.0 : p.mass);
     a.soft = p.soften;
     a.r_soft = 1.0 / p.soften;

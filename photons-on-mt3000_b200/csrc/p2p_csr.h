@@ -22,6 +22,9 @@ struct CsrBufs {
     int64_t *hsums = nullptr;           // csr_hsum_len(ntask)
     unsigned long long *pairs = nullptr;  // += pair count
     int *status = nullptr;              // |= ST_* bits
+    unsigned long long *skipped = nullptr;  // += pairs of entries wholly beyond the cutoff (nullable)
+    double cscale = 1.0;                // frame scale and bound used for skipped
+    float uout = 0.f;
 };
 
 inline int csr_grid(int64_t n, int threads, int cap_blocks) {
@@ -45,8 +48,8 @@ inline cudaError_t enqueue_csr_build(cudaStream_t st, int64_t ntask, const int *
     const int threads = 256;
     cudaError_t e = cudaMemsetAsync(b.counts, 0, sizeof(int) * (size_t)nleaf, st);
     if (e != cudaSuccess) return e;
-    csr_count_kernel<<<csr_grid(ntask, threads, 148 * 16), threads, 0, st>>>(d_t, d_s, ntask, nleaf, meta,
-                                                                             b.counts, b.pairs, b.status);
+    csr_count_kernel<<<csr_grid(ntask, threads, 148 * 16), threads, 0, st>>>(
+        d_t, d_s, ntask, nleaf, meta, b.counts, b.pairs, b.status, b.skipped, b.cscale, b.uout);
     const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
     scan_tiles_kernel<<<ntiles, kScanThreads, 0, st>>>(b.counts, nleaf, b.row_off, b.tile_sums);
     scan_sums_kernel<<<1, kScanThreads, 0, st>>>(b.tile_sums, ntiles, b.row_off + nleaf);

@@ -31,6 +31,9 @@ constexpr double kCutBand = 1.0e-5;
 // Entries whose bound on u is below x_cut^2 (1 - kInsideMargin) cannot hold a
 // band pair; the margin covers the FP32 rounding of the bound itself.
 constexpr double kInsideMargin = 5.0e-5;
+// Entries whose lower bound on u exceeds x_cut^2 (1 + kCutBand)(1 + kOutsideMargin)
+// hold no pair the FP32 forms keep; the margin covers the FP32 rounding of the bound.
+constexpr double kOutsideMargin = 5.0e-5;
 // Default bound on x |dH| of the fitted polynomial.
 constexpr double kDefaultPolyTol = 1.0e-7;
 
@@ -65,6 +68,7 @@ struct PairArgs {
     float2 coef2[kMaxCoef];  // (coef[k], coef[k]): packed f32x2 operands straight from the constant bank
     float2 eps2_2, negu0_2;  // (eps2, eps2), (-u0, -u0)
     float uin;               // entries whose bound on u stays below uin hold no cutoff-band pair
+    float uout;              // entries whose lower bound on u exceeds uout hold no kept pair
     // FP64 form (reference units)
     double soft, r_soft, hrrs, rrs, coeff, xcut, mass_eq;
     // Packed launches over several resident boxes (nseg > 0): work items

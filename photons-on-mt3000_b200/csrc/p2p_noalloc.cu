@@ -237,7 +237,7 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
             d_leaf_ipart, d_leaf_npart, npart, nleaf, meta, status);
     const int eblocks = grid_cap(ntask, threads, sms * 16);
     csr_count_kernel<<<eblocks, threads, 0, s>>>(d_task_t, d_task_s, ntask, nleaf, meta, counts,
-                                                 pairs, status);
+                                                 pairs, status, nullptr, 1.0, 0.f);
     const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
     scan_tiles_kernel<<<ntiles, kScanThreads, 0, s>>>(counts, nleaf, row_off, tiles);
     scan_sums_kernel<<<1, kScanThreads, 0, s>>>(tiles, ntiles, row_off + nleaf);

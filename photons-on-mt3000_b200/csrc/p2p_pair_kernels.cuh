@@ -574,15 +574,11 @@ __device__ __forceinline__ void stage_row_flat(const PairArgs &a, const LeafMeta
         if (lane < ne) {
             const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
             sip = ms.ipart;
-            snp = ms.npart;
-            ox = (float)((ms.cx - mt.cx) * a.cscale);
-            oy = (float)((ms.cy - mt.cy) * a.cscale);
-            oz = (float)((ms.cz - mt.cz) * a.cscale);
-            // largest u any pair of this entry can reach (box bound)
-            const float bx = fabsf(ox) + ms.hx + mt.hx, by = fabsf(oy) + ms.hy + mt.hy,
-                        bz = fabsf(oz) + ms.hz + mt.hz;
-            const float umax_entry = fmaf(bx, bx, fmaf(by, by, fmaf(bz, bz, a.eps2)));
-            chk = umax_entry < a.uin ? 0 : (int)0x80000000;
+            entry_offset(ms, mt, a.cscale, ox, oy, oz);
+            // entries wholly beyond the cutoff are not staged (their pairs would
+            // all be dropped); the others take the cutoff test unless wholly inside
+            snp = entry_u_min(ms, mt, ox, oy, oz) > a.uout ? 0 : ms.npart;
+            chk = entry_u_max(ms, mt, ox, oy, oz, a.eps2) < a.uin ? 0 : (int)0x80000000;
         }
         int incl = snp;  // inclusive prefix sum of the entries' sizes
 #pragma unroll

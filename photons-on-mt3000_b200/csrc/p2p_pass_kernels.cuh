@@ -104,14 +104,17 @@ __global__ void prep_plain_kernel(const int *__restrict__ leaf_ip, const int *__
 
 // ----------------------------------------------------------------- CSR ----
 
+// skipped (nullable): += pairs of entries the FP32 pair kernels skip as lying
+// wholly beyond the cutoff (lower bound on u above uout, frames scaled by cscale).
 __global__ void csr_count_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,
                                  int nleaf, const LeafMeta *__restrict__ meta,
                                  int *__restrict__ counts, unsigned long long *__restrict__ pairs,
-                                 int *__restrict__ status) {
-    __shared__ unsigned long long block_pairs;
-    if (threadIdx.x == 0) block_pairs = 0;
+                                 int *__restrict__ status, unsigned long long *__restrict__ skipped,
+                                 double cscale, float uout) {
+    __shared__ unsigned long long block_pairs, block_skip;
+    if (threadIdx.x == 0) block_pairs = block_skip = 0;
     __syncthreads();
-    unsigned long long local = 0;
+    unsigned long long local = 0, lskip = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
         const int t = tt[e], s = ts[e];
@@ -120,13 +123,25 @@ __global__ void csr_count_kernel(const int *__restrict__ tt, const int *__restri
             continue;
         }
         atomicAdd(&counts[t], 1);
-        local += (unsigned long long)meta[t].npart * (unsigned long long)meta[s].npart;
+        const LeafMeta mt = meta[t], ms = meta[s];
+        const unsigned long long np = (unsigned long long)mt.npart * (unsigned long long)ms.npart;
+        local += np;
+        if (skipped) {
+            float ox, oy, oz;
+            entry_offset(ms, mt, cscale, ox, oy, oz);
+            if (entry_u_min(ms, mt, ox, oy, oz) > uout) lskip += np;
+        }
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) local += __shfl_xor_sync(kFull, local, off);
+    for (int off = 16; off > 0; off >>= 1) {
+        local += __shfl_xor_sync(kFull, local, off);
+        lskip += __shfl_xor_sync(kFull, lskip, off);
+    }
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(&block_pairs, local);
+    if ((threadIdx.x & 31) == 0 && lskip) atomicAdd(&block_skip, lskip);
     __syncthreads();
     if (threadIdx.x == 0 && block_pairs) atomicAdd(pairs, block_pairs);
+    if (threadIdx.x == 0 && block_skip) atomicAdd(skipped, block_skip);
 }
 
 __global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__restrict__ ts, int64_t n,

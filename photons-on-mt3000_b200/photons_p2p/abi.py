@@ -107,6 +107,7 @@ SIGNATURES = {
     "p2p_pass_result_device": (_i, [_vp, ctypes.POINTER(_vp)]),
     "p2p_session_synchronize": (_i, [_vp]),
     "p2p_pass_pair_count": (_i, [_vp, ctypes.POINTER(_i64)]),
+    "p2p_pass_evaluated_pairs": (_i, [_vp, ctypes.POINTER(_i64)]),
     "p2p_pass_run_device": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i64, _vp, _vp]),
     "p2p_kernel_launch_count": (_i64, []),
     "p2p_session_last_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),

@@ -120,6 +120,13 @@ class Session:
         _check(self.lib, self.lib.p2p_pass_pair_count(self.h, ctypes.byref(v)))
         return v.value
 
+    def evaluated_pairs(self):
+        """Pair interactions the kernels evaluated in the current pass (the
+        listed ones minus those of entries skipped as wholly beyond the cutoff)."""
+        v = ctypes.c_int64()
+        _check(self.lib, self.lib.p2p_pass_evaluated_pairs(self.h, ctypes.byref(v)))
+        return v.value
+
     def last_kernel_ms(self):
         v = ctypes.c_float()
         _check(self.lib, self.lib.p2p_session_last_kernel_ms(self.h, ctypes.byref(v)))
