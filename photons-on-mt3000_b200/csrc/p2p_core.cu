@@ -578,10 +578,11 @@ P2P_API int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, co
     if (ntask < 0) return fail(P2P_ERR_ARG, "negative ntask");
     if (ntask == 0) return P2P_OK;
     if (!task_t || !task_s) return fail(P2P_ERR_ARG, "null task list");
-    if (ntask > 2 * kPipePieceMin) {
-        // Large lists: upload in pieces on the copy stream while the previous
-        // piece's CSR build and pair kernel run (each piece is a list chunk,
-        // as the reference's LEN_TASK chunks are).
+    if (ntask > 2 * kPipePieceMin && is_fp32_form(s->params.form)) {
+        // Large lists (FP32 forms): upload in pieces on the copy stream while
+        // the previous piece's CSR build and pair kernel run (each piece is a
+        // list chunk, as the reference's LEN_TASK chunks are). The FP64 form
+        // keeps one chunk: its slowest rows would stretch every piece's tail.
         const int64_t piece = std::max<int64_t>(kPipePieceMin, (ntask + kPipePieces - 1) / kPipePieces);
         P2P_TRY(ensure(s, s->task_t, sizeof(int) * (size_t)piece));
         P2P_TRY(ensure(s, s->task_s, sizeof(int) * (size_t)piece));

@@ -415,6 +415,9 @@ struct SinkPair {
 #ifndef P2P_X2_TWO_SOURCES
 #define P2P_X2_TWO_SOURCES 0  // two staged sources per lane per step
 #endif
+#ifndef P2P_X2_S16_MINBLOCKS
+#define P2P_X2_S16_MINBLOCKS 4  // resident blocks per SM the 16-sink tile's register budget targets
+#endif
 #ifndef P2P_X2_SINKPAIRS
 #define P2P_X2_SINKPAIRS 16  // sink pairs per slice (a slice holds 2x that many sinks)
 #endif
@@ -622,7 +625,7 @@ __device__ __forceinline__ void stage_row_flat(const PairArgs &a, const LeafMeta
 // NP sink pairs per slice: 16 (32-sink tile, 3 blocks of 4 warps per SM) or
 // 8 (16-sink tile, half the partial registers, 4 blocks per SM).
 template <int SOFT, bool MASSES, int ACC, int NC, int NP = P2P_X2_SINKPAIRS>
-__global__ void __launch_bounds__(128, NP == 8 ? 4 : P2P_X2_MINBLOCKS)
+__global__ void __launch_bounds__(128, NP == 8 ? P2P_X2_S16_MINBLOCKS : P2P_X2_MINBLOCKS)
 pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
     extern __shared__ float4 smem_f4[];
     using Acc = typename AccSel<ACC>::T;
