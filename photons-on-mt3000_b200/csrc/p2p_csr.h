@@ -56,28 +56,39 @@ inline cudaError_t enqueue_csr_build(cudaStream_t st, int64_t ntask, const int *
     scan_add_kernel<<<csr_grid(nleaf, threads, 1 << 30), threads, 0, st>>>(b.row_off, nleaf, b.tile_sums);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     *launches += 4;
-    // radix passes over keys in [0, nleaf]
+    // radix passes over keys in [0, nleaf]: 8-bit digits, or two 10-bit
+    // digits for 17-20 key bits (one pass fewer)
     int bits = 1;
     while (bits < 31 && ((int64_t)1 << bits) <= (int64_t)nleaf) ++bits;
-    const int passes = (bits + 7) / 8;
     const int rtiles = (int)((ntask + kRadixTile - 1) / kRadixTile);
-    const int nh = kRadixBins * rtiles;
+    // (the 10-bit histogram of more than 2^20 tiles would overflow int)
+    const int digit = (bits > 16 && bits <= 20 && rtiles <= (1 << 20)) ? 10 : 8;
+    const int passes = (bits + digit - 1) / digit;
+    const int nh = (1 << digit) * rtiles;
     const int hscan_tiles = (nh + kScanTile - 1) / kScanTile;
     int *kbuf[2] = {b.keys_a, b.keys_b};
     int *vbuf[2] = {b.row_src, b.vals_b};
     const int *kin = nullptr, *vin = nullptr;
     for (int pass = 0; pass < passes; ++pass) {
-        const int shift = 8 * pass;
+        const int shift = digit * pass;
         const int o = (passes - 1 - pass) & 1;  // the last pass lands in row_src
         int *kout = pass == passes - 1 ? nullptr : kbuf[o];
         int *vout = vbuf[o];
-        radix_hist_kernel<<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask, shift, b.hist,
-                                                               rtiles);
+        if (digit == 10)
+            radix_hist_kernel<10><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask, shift,
+                                                                       b.hist, rtiles);
+        else
+            radix_hist_kernel<8><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask, shift,
+                                                                      b.hist, rtiles);
         scan_tiles_kernel<<<hscan_tiles, kScanThreads, 0, st>>>(b.hist, nh, b.hoffs, b.hsums);
         scan_sums_kernel<<<1, kScanThreads, 0, st>>>(b.hsums, hscan_tiles, b.hoffs + nh);
         scan_add_kernel<<<csr_grid(nh, 256, 1 << 30), 256, 0, st>>>(b.hoffs, nh, b.hsums);
-        radix_scatter_kernel<<<rtiles, kRadixWarps * 32, 0, st>>>(kin, vin, d_t, d_s, nleaf, ntask, shift,
-                                                                  b.hoffs, rtiles, kout, vout);
+        if (digit == 10)
+            radix_scatter_kernel<10><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, vin, d_t, d_s, nleaf, ntask, shift,
+                                                                          b.hoffs, rtiles, kout, vout);
+        else
+            radix_scatter_kernel<8><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, vin, d_t, d_s, nleaf, ntask, shift,
+                                                                         b.hoffs, rtiles, kout, vout);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         *launches += 5;
         kin = kout;

@@ -255,7 +255,7 @@ csr_sort_rows_global_kernel(const int64_t *__restrict__ row_off, int nleaf, int 
 // radix_scatter_kernel (stable rank of each entry within its tile by digit,
 // from warp-private counts and __match_any_sync, then the scatter). Entries
 // with an out-of-range sink or source get key nleaf and sort past the rows.
-constexpr int kRadixBins = 256;
+constexpr int kRadixBins = 1024;  // most bins of a digit (10 bits); histograms are sized for it
 constexpr int kRadixWarps = 8;
 constexpr int kRadixRounds = 16;
 constexpr int kRadixTile = kRadixWarps * kRadixRounds * 32;  // 4096 entries
@@ -268,22 +268,26 @@ __device__ __forceinline__ unsigned radix_key(const int *keys, const int *raw_t,
 }
 
 // keys == nullptr: first pass, keys computed from the raw (t, s) list.
+// BITS: digit width (8 or 10).
+template <int BITS>
 __global__ void __launch_bounds__(kRadixWarps * 32)
 radix_hist_kernel(const int *__restrict__ keys, const int *__restrict__ raw_t,
                   const int *__restrict__ raw_s, int nleaf, int64_t n, int shift,
                   int *__restrict__ hist, int ntiles) {
-    __shared__ int h[kRadixWarps][kRadixBins];
+    constexpr int NB = 1 << BITS;
+    constexpr unsigned MASK = NB - 1u;
+    __shared__ int h[kRadixWarps][NB];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int b = threadIdx.x; b < kRadixWarps * kRadixBins; b += blockDim.x) (&h[0][0])[b] = 0;
+    for (int b = threadIdx.x; b < kRadixWarps * NB; b += blockDim.x) (&h[0][0])[b] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kRadixTile + (int64_t)w * kRadixRounds * 32;
 #pragma unroll 4
     for (int r = 0; r < kRadixRounds; ++r) {
         const int64_t i = base + r * 32 + lane;
-        if (i < n) atomicAdd(&h[w][(radix_key(keys, raw_t, raw_s, nleaf, i) >> shift) & 255u], 1);
+        if (i < n) atomicAdd(&h[w][(radix_key(keys, raw_t, raw_s, nleaf, i) >> shift) & MASK], 1);
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < kRadixBins; b += blockDim.x) {
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) {
         int tot = 0;
 #pragma unroll
         for (int q = 0; q < kRadixWarps; ++q) tot += h[q][b];
@@ -291,17 +295,20 @@ radix_hist_kernel(const int *__restrict__ keys, const int *__restrict__ raw_t,
     }
 }
 
+template <int BITS>
 __global__ void __launch_bounds__(kRadixWarps * 32)
 radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
                      const int *__restrict__ raw_t, const int *__restrict__ raw_s, int nleaf,
                      int64_t n, int shift, const int64_t *__restrict__ offs, int ntiles,
                      int *__restrict__ keys_out, int *__restrict__ vals_out) {
-    __shared__ int cnt[kRadixWarps][kRadixBins];
-    __shared__ int64_t gbase[kRadixBins];
+    constexpr int NB = 1 << BITS;
+    constexpr unsigned MASK = NB - 1u;
+    __shared__ int cnt[kRadixWarps][NB];
+    __shared__ int64_t gbase[NB];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    for (int b = threadIdx.x; b < kRadixWarps * kRadixBins; b += blockDim.x) (&cnt[0][0])[b] = 0;
-    for (int b = threadIdx.x; b < kRadixBins; b += blockDim.x)
+    for (int b = threadIdx.x; b < kRadixWarps * NB; b += blockDim.x) (&cnt[0][0])[b] = 0;
+    for (int b = threadIdx.x; b < NB; b += blockDim.x)
         gbase[b] = offs[(int64_t)b * ntiles + blockIdx.x];
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kRadixTile + (int64_t)w * kRadixRounds * 32;
@@ -314,14 +321,14 @@ radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
         const bool ok = i < n;
         key[r] = ok ? radix_key(keys, raw_t, raw_s, nleaf, i) : 0xffffffffu;
         val[r] = ok ? (vals ? vals[i] : raw_s[i]) : 0;
-        const int d = ok ? (int)((key[r] >> shift) & 255u) : 256 + lane;  // tail lanes: own group
+        const int d = ok ? (int)((key[r] >> shift) & MASK) : NB + lane;  // tail lanes: own group
         peers[r] = __match_any_sync(kFull, d);
         if (ok && lane == __ffs(peers[r]) - 1) cnt[w][d] += __popc(peers[r]);
         __syncwarp();
     }
     __syncthreads();
     // exclusive base of every warp within the tile, per bin
-    for (int b = threadIdx.x; b < kRadixBins; b += blockDim.x) {
+    for (int b = threadIdx.x; b < NB; b += blockDim.x) {
         int run = 0;
 #pragma unroll
         for (int q = 0; q < kRadixWarps; ++q) {
@@ -335,7 +342,7 @@ radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
     for (int r = 0; r < kRadixRounds; ++r) {
         const int64_t i = base + r * 32 + lane;
         const bool ok = i < n;
-        const int d = ok ? (int)((key[r] >> shift) & 255u) : 0;
+        const int d = ok ? (int)((key[r] >> shift) & MASK) : 0;
         const int before = ok ? cnt[w][d] : 0;
         __syncwarp();
         if (ok) {

@@ -309,3 +309,26 @@ def test_pipelined_host_submit_matches_resident_pass(gpu):
         s.accumulate(ref)
     rms, mx = rel_err(got, ref, tl.tag == 1)
     assert rms <= 1e-6 and mx <= 1e-4, (rms, mx)
+
+
+def test_plain_matches_oracle_with_ten_bit_radix(gpu):
+    """More than 2^16 leaves: the CSR build sorts with two 10-bit radix digits.
+    The rows of every 97th sink leaf of a 128^3 clustered pass, through the
+    plain FP64 form, against the reference-order oracle."""
+    side = 128
+    cfg = W.scaled(W.c2_config(), n_side=side, mesh=side, eps=1 / (40 * side))
+    tl = W.prepare(W.c2_positions(side), cfg)
+    assert 2 ** 16 <= tl.nleaf < 2 ** 20
+    keep = (tl.task_t % 97) == 0
+    tt, ts = tl.task_t[keep], tl.task_s[keep]
+    mass = 1.0 / int(tl.tag.sum())
+    prm = O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass)
+    ref, pairs = O.p2p_lists(prm, tl.pos, tl.leaf_ipart, tl.leaf_npart, tt, ts)
+    with Session(gpu, params_for(cfg, abi.FORM_PLAIN_FP64, mass)) as s:
+        got, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tt, ts)
+        assert s.pair_count() == pairs
+    sinks = np.zeros(tl.npart, bool)
+    for l in np.unique(tt):
+        sinks[tl.leaf_ipart[l]:tl.leaf_ipart[l] + tl.leaf_npart[l]] = True
+    rms, mx = rel_err(got, ref, sinks)
+    assert mx <= PLAIN_MAX, mx
