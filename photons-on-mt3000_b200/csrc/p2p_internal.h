@@ -65,8 +65,6 @@ struct PairArgs {
     double cscale;           // c
     double out_scale;        // c^2 * mass (equal masses) or c^2 (per-particle masses)
     float coef[kMaxCoef];    // -H(u) ~ sum coef[k] (u - u0)^k (negated, so f = rinv^2 * rinv + poly)
-    float2 coef2[kMaxCoef];  // (coef[k], coef[k]): packed f32x2 operands straight from the constant bank
-    float2 eps2_2, negu0_2;  // (eps2, eps2), (-u0, -u0)
     float uin;               // entries whose bound on u stays below uin hold no cutoff-band pair
     float uout;              // entries whose lower bound on u exceeds uout hold no kept pair
     // FP64 form (reference units)

@@ -394,26 +394,8 @@ struct SinkPair {
 #ifndef P2P_X2_GROUP
 #define P2P_X2_GROUP 4  // packed sink pairs per predicated block (8 sinks)
 #endif
-#ifndef P2P_X2_SCALAR_POLY
-#define P2P_X2_SCALAR_POLY 0  // 1: polynomial as two scalar Horner chains (measured slower)
-#endif
-#ifndef P2P_X2_ESTRIN
-#define P2P_X2_ESTRIN 0  // otherwise packed: Estrin's scheme (1) or Horner's rule (0)
-#endif
 #ifndef P2P_X2_MINBLOCKS
 #define P2P_X2_MINBLOCKS 3  // resident 128-thread blocks per SM the register budget targets
-#endif
-#ifndef P2P_X2_HOIST_COEF
-#define P2P_X2_HOIST_COEF 0  // packed coefficient pairs held in registers for the whole kernel
-#endif
-#ifndef P2P_X2_COEF_PAIRS
-#define P2P_X2_COEF_PAIRS 0  // packed coefficient pairs from the parameters (no duplication per use)
-#endif
-#ifndef P2P_X2_ALWAYS_CHECK
-#define P2P_X2_ALWAYS_CHECK 0  // one code path: every chunk takes the cutoff select and band test
-#endif
-#ifndef P2P_X2_TWO_SOURCES
-#define P2P_X2_TWO_SOURCES 0  // two staged sources per lane per step
 #endif
 #ifndef P2P_X2_S16_MINBLOCKS
 #define P2P_X2_S16_MINBLOCKS 4  // resident blocks per SM the 16-sink tile's register budget targets
@@ -423,64 +405,15 @@ struct SinkPair {
 #endif
 constexpr int kPairGroup = P2P_X2_GROUP;
 
-// H(t) for two sinks at once. Horner: one packed FMA per coefficient.
-// Estrin: the first layer c_{2j} + c_{2j+1} t runs as scalar FMAs (their
-// constants are free instruction operands), the upper layers combine with
-// powers t^2, t^4, t^8 in packed FMAs; the dependency depth drops from NC-1
-// to about log2(NC) + 1.
+// H(t) for two sinks at once: Horner's rule, one packed FMA per coefficient.
+// (Measured alternatives: two scalar Horner chains, Estrin's scheme,
+// coefficient pairs held in registers or read as f32x2 parameters.)
 template <int NC>
-__device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a, const float2 *cv) {
-#if P2P_X2_SCALAR_POLY
-    // two scalar Horner chains: coefficients stay constant-bank operands
-    float hx = a.coef[NC - 1], hy = a.coef[NC - 1];
-#pragma unroll
-    for (int k = NC - 2; k >= 0; --k) {
-        hx = fmaf(hx, t.x, a.coef[k]);
-        hy = fmaf(hy, t.y, a.coef[k]);
-    }
-    return make_float2(hx, hy);
-#elif P2P_X2_ESTRIN
-    constexpr int NQ = (NC + 1) / 2;  // first-layer terms
-    float2 q[NQ];
-#pragma unroll
-    for (int j = 0; j < NQ; ++j) {
-        if (2 * j + 1 < NC) {
-            q[j].x = fmaf(a.coef[2 * j + 1], t.x, a.coef[2 * j]);
-            q[j].y = fmaf(a.coef[2 * j + 1], t.y, a.coef[2 * j]);
-        } else {
-            q[j] = make_float2(a.coef[2 * j], a.coef[2 * j]);
-        }
-    }
-    float2 pw = __fmul2_rn(t, t);  // t^2, then t^4, t^8, ...
-    int n = NQ;
-#pragma unroll
-    for (int level = 0; level < 5; ++level) {
-        if (n > 1) {
-#pragma unroll
-            for (int j = 0; j < n / 2; ++j) q[j] = __ffma2_rn(q[2 * j + 1], pw, q[2 * j]);
-            if (n & 1) q[n / 2] = q[n - 1];
-            n = (n + 1) / 2;
-            if (n > 1) pw = __fmul2_rn(pw, pw);
-        }
-    }
-    return q[0];
-#elif P2P_X2_HOIST_COEF
-    float2 h = cv[NC - 1];
-#pragma unroll
-    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, cv[k]);
-    return h;
-#elif P2P_X2_COEF_PAIRS
-    // packed coefficient pairs read from the kernel parameters
-    float2 h = a.coef2[NC - 1];
-#pragma unroll
-    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, a.coef2[k]);
-    return h;
-#else
+__device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
     float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);
 #pragma unroll
     for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, make_float2(a.coef[k], a.coef[k]));
     return h;
-#endif
 }
 
 // CHECK = false: every pair is known to be inside the cutoff (no select).
@@ -490,7 +423,7 @@ template <int SOFT, bool MASSES, int NC, bool CHECK>
 __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
                                               const float sw, const SinkPair &p,
                                               const PairArgs &a, const float2 eps2v,
-                                              const float2 negu0v, const float2 *cv, float2 &ax, float2 &ay,
+                                              const float2 negu0v, float2 &ax, float2 &ay,
                                               float2 &az, bool &amb) {
     const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
     const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
@@ -505,7 +438,7 @@ __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, 
     }
     const float2 r = make_float2(rsqrt_approx(u.x), rsqrt_approx(u.y));
     const float2 t = __fadd2_rn(u, negu0v);
-    const float2 h = poly_x2<NC>(t, a, cv);  // -H(u)
+    const float2 h = poly_x2<NC>(t, a);  // -H(u)
     float2 f = __ffma2_rn(__fmul2_rn(r, r), r, h);
     if (CHECK) {
         const bool in_x = u.x <= a.ucut_lo, in_y = u.y <= a.ucut_lo;
@@ -549,13 +482,6 @@ __device__ __forceinline__ bool band_pair(const float4 src, const float psx, con
     return true;
 }
 
-#ifndef P2P_STAGE_UNROLL
-#define P2P_STAGE_UNROLL 1  // rounds of 32 staged sources unrolled (loads of several rounds in flight)
-#endif
-constexpr int kStageUnroll = P2P_STAGE_UNROLL;
-#ifndef P2P_FLAT_STAGE
-#define P2P_FLAT_STAGE 1  // stage a row's sources with all lanes' loads in flight at once
-#endif
 
 // Stages the sources of row entries [rb, re) of sink leaf mt: each source
 // leaf's FP32 coordinates shifted into the sink's frame by the FP32-rounded
@@ -594,7 +520,6 @@ __device__ __forceinline__ void stage_row_flat(const PairArgs &a, const LeafMeta
         while (done < total) {
             if (fill == stage_cap) consume();
             const int take = min(total - done, stage_cap - fill);
-#pragma unroll kStageUnroll
             for (int t0 = 0; t0 < take; t0 += 32) {
                 const int t = t0 + lane;
                 const int g = done + min(t, take - 1);  // this lane's source (idle lanes repeat the last)
@@ -640,9 +565,6 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
     float4 *stage = region + 64;
     int *sidx = reinterpret_cast<int *>(stage + stage_cap);
     const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
-    float2 cv[NC];  // packed coefficient pairs (used when P2P_X2_HOIST_COEF)
-#pragma unroll
-    for (int k = 0; k < NC; ++k) cv[k] = make_float2(a.coef[k], a.coef[k]);
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1);
@@ -689,50 +611,6 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
             auto consume = [&]() {
                 __syncwarp();
                 unsigned ambmask = 0;  // chunks of this batch with a pair in the cutoff band
-#if P2P_X2_TWO_SOURCES
-                // two staged sources per lane per step: twice the independent
-                // dependency chains for the same sink pairs
-                for (int c = 0, ci = 0; c < fill; c += 64, ci += 2) {
-                    const int slot0 = c + lane, slot1 = c + 32 + lane;
-                    const float4 far = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
-                    const float4 s0 = slot0 < fill ? stage[slot0] : far;
-                    const float4 s1 = slot1 < fill ? stage[slot1] : far;
-                    const float2 sx0 = make_float2(s0.x, s0.x), sy0 = make_float2(s0.y, s0.y),
-                                 sz0 = make_float2(s0.z, s0.z);
-                    const float2 sx1 = make_float2(s1.x, s1.x), sy1 = make_float2(s1.y, s1.y),
-                                 sz1 = make_float2(s1.z, s1.z);
-                    const bool check = __any_sync(kFull, slot1 >= fill || sidx[slot0] < 0 || sidx[slot1] < 0);
-                    bool amb0 = false, amb1 = false;
-                    if (check) {
-#pragma unroll
-                        for (int g = 0; g < NP; g += kPairGroup) {
-                            if (2 * g < ns) {
-#pragma unroll
-                                for (int q = 0; q < kPairGroup; ++q) {
-                                    pair_split_x2<SOFT, MASSES, NC, true>(sx0, sy0, sz0, s0.w, sinks[g + q], a, eps2v,
-                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb0);
-                                    pair_split_x2<SOFT, MASSES, NC, true>(sx1, sy1, sz1, s1.w, sinks[g + q], a, eps2v,
-                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb1);
-                                }
-                            }
-                        }
-                    } else {
-#pragma unroll
-                        for (int g = 0; g < NP; g += kPairGroup) {
-                            if (2 * g < ns) {
-#pragma unroll
-                                for (int q = 0; q < kPairGroup; ++q) {
-                                    pair_split_x2<SOFT, MASSES, NC, false>(sx0, sy0, sz0, s0.w, sinks[g + q], a, eps2v,
-                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb0);
-                                    pair_split_x2<SOFT, MASSES, NC, false>(sx1, sy1, sz1, s1.w, sinks[g + q], a, eps2v,
-                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb1);
-                                }
-                            }
-                        }
-                    }
-                    ambmask |= (amb0 ? (1u << ci) : 0u) | (amb1 ? (2u << ci) : 0u);
-                }
-#else
                 for (int c = 0, ci = 0; c < fill; c += 32, ++ci) {
                     const int slot = c + lane;
                     const float4 src = slot < fill ? stage[slot]
@@ -741,11 +619,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                                  sz = make_float2(src.z, src.z);
                     // full chunks whose sources all come from entries inside the
                     // cutoff skip the select and the band test
-#if P2P_X2_ALWAYS_CHECK
-                    const bool check = true;
-#else
                     const bool check = __any_sync(kFull, slot >= fill || sidx[slot] < 0);
-#endif
                     bool amb = false;
                     if (check) {
 #pragma unroll
@@ -754,7 +628,7 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
                                     pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                          negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb);
+                                                                          negu0v, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     } else {
@@ -764,13 +638,12 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
 #pragma unroll
                                 for (int q = 0; q < kPairGroup; ++q)
                                     pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                           negu0v, cv, ax[g + q], ay[g + q], az[g + q], amb);
+                                                                           negu0v, ax[g + q], ay[g + q], az[g + q], amb);
                             }
                         }
                     }
                     ambmask |= amb ? (1u << ci) : 0u;
                 }
-#endif
                 // rare: pairs within the cutoff band, decided in FP64
                 if (__any_sync(kFull, ambmask != 0u)) {
                     while (ambmask) {
@@ -799,53 +672,12 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                 fill = 0;
                 if (chunks >= kSrcFlushChunks) flush();
             };
-#if P2P_FLAT_STAGE
             stage_row_flat(a, mt, rb, re, lane, stage_cap, fill,
                            [&](int slot, const float4 v, int idx) {
                                stage[slot] = v;
                                sidx[slot] = idx;
                            },
                            consume);
-#else
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0, chk = 0;
-                float ox = 0.f, oy = 0.f, oz = 0.f;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                    ox = (float)((ms.cx - mt.cx) * a.cscale);
-                    oy = (float)((ms.cy - mt.cy) * a.cscale);
-                    oz = (float)((ms.cz - mt.cz) * a.cscale);
-                    // largest u any pair of this entry can reach (box bound)
-                    const float bx = fabsf(ox) + ms.hx + mt.hx, by = fabsf(oy) + ms.hy + mt.hy,
-                                bz = fabsf(oz) + ms.hz + mt.hz;
-                    const float umax_entry = fmaf(bx, bx, fmaf(by, by, fmaf(bz, bz, a.eps2)));
-                    chk = umax_entry < a.uin ? 0 : (int)0x80000000;
-                }
-                for (int j = 0; j < ne; ++j) {
-                    const int jnp = __shfl_sync(kFull, snp, j);
-                    const int jip = __shfl_sync(kFull, sip, j);
-                    const int jchk = __shfl_sync(kFull, chk, j);
-                    const float jx = __shfl_sync(kFull, ox, j);
-                    const float jy = __shfl_sync(kFull, oy, j);
-                    const float jz = __shfl_sync(kFull, oz, j);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) consume();
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const float4 v = a.pos4[jip + q0 + q];
-                            stage[fill + q] = make_float4(v.x + jx, v.y + jy, v.z + jz, v.w);
-                            sidx[fill + q] = (jip + q0 + q) | jchk;
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-#endif
             if (fill) consume();
             if (chunks) flush();
             __syncwarp();  // sinks[] and corr[] are rewritten by the next slice
@@ -887,9 +719,6 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
     float4 *stage = smem_f4 + (threadIdx.x >> 5) * (2 * cap + cap / 4);
     int *sidx = reinterpret_cast<int *>(stage + 2 * cap);
     const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
-    float2 cv[NC];
-#pragma unroll
-    for (int k = 0; k < NC; ++k) cv[k] = make_float2(a.coef[k], a.coef[k]);
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1);
@@ -942,10 +771,10 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                                      sz = make_float2(B.x, B.y);
                         bool amb = false;
                         if (__any_sync(kFull, owner && sid < 0))
-                            pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
+                            pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, ax, ay,
                                                                   az, amb);
                         else
-                            pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, cv, ax, ay,
+                            pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, B.z, sp, a, eps2v, negu0v, ax, ay,
                                                                    az, amb);
                         ambbits |= amb ? (1u << k) : 0u;
                     }
@@ -984,7 +813,6 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                 __syncwarp();
             };
             int fill = 0;
-#if P2P_FLAT_STAGE
             stage_row_flat(a, mt, rb, re, lane, stage_cap, fill,
                            [&](int slot, const float4 v, int idx) {
                                stage[2 * slot] = make_float4(v.x, v.x, v.y, v.y);
@@ -995,50 +823,6 @@ pair_sink2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
                                consume(fill);
                                fill = 0;
                            });
-#else
-            for (int64_t e0 = rb; e0 < re; e0 += 32) {
-                const int ne = (int)min((int64_t)32, re - e0);
-                int sip = 0, snp = 0, chk = 0;
-                float ox = 0.f, oy = 0.f, oz = 0.f;
-                if (lane < ne) {
-                    const LeafMeta ms = a.leaf[a.row_src[e0 + lane]];
-                    sip = ms.ipart;
-                    snp = ms.npart;
-                    ox = (float)((ms.cx - mt.cx) * a.cscale);
-                    oy = (float)((ms.cy - mt.cy) * a.cscale);
-                    oz = (float)((ms.cz - mt.cz) * a.cscale);
-                    const float bx = fabsf(ox) + ms.hx + mt.hx, by = fabsf(oy) + ms.hy + mt.hy,
-                                bz = fabsf(oz) + ms.hz + mt.hz;
-                    const float umax_entry = fmaf(bx, bx, fmaf(by, by, fmaf(bz, bz, a.eps2)));
-                    chk = umax_entry < a.uin ? 0 : (int)0x80000000;
-                }
-                for (int jj = 0; jj < ne; ++jj) {
-                    const int jnp = __shfl_sync(kFull, snp, jj);
-                    const int jip = __shfl_sync(kFull, sip, jj);
-                    const int jchk = __shfl_sync(kFull, chk, jj);
-                    const float jx = __shfl_sync(kFull, ox, jj);
-                    const float jy = __shfl_sync(kFull, oy, jj);
-                    const float jz = __shfl_sync(kFull, oz, jj);
-                    int q0 = 0;
-                    while (q0 < jnp) {
-                        if (fill == stage_cap) {
-                            consume(fill);
-                            fill = 0;
-                        }
-                        const int take = min(jnp - q0, stage_cap - fill);
-                        for (int q = lane; q < take; q += 32) {
-                            const float4 v = a.pos4[jip + q0 + q];
-                            const float x = v.x + jx, y = v.y + jy, z = v.z + jz;
-                            stage[2 * (fill + q)] = make_float4(x, x, y, y);
-                            stage[2 * (fill + q) + 1] = make_float4(z, z, v.w, v.w);
-                            sidx[fill + q] = (jip + q0 + q) | jchk;
-                        }
-                        fill += take;
-                        q0 += take;
-                    }
-                }
-            }
-#endif
             if (fill) consume(fill);
             acc_a.add(ax.x, ay.x, az.x);
             acc_b.add(ax.y, ay.y, az.y);
