@@ -38,7 +38,11 @@ inline size_t csr_hist_len(int64_t ntask) {
     const int64_t n = std::max<int64_t>(ntask, 1);
     return (size_t)kRadixBins * (size_t)((n + kRadixTile - 1) / kRadixTile);
 }
-inline size_t csr_hsum_len(int64_t ntask) { return (csr_hist_len(ntask) + kScanTile - 1) / kScanTile + 1; }
+inline size_t csr_hsum_len(int64_t ntask) {  // chunk sums of the histogram's column scan
+    const int64_t n = std::max<int64_t>(ntask, 1);
+    const int64_t rtiles = (n + kRadixTile - 1) / kRadixTile;
+    return (size_t)kRadixBins * (size_t)((rtiles + kColTiles - 1) / kColTiles) + 1;
+}
 
 // Enqueues the build on `st`; *launches += kernels launched.
 inline cudaError_t enqueue_csr_build(cudaStream_t st, int64_t ntask, const int *d_t, const int *d_s,
@@ -61,11 +65,10 @@ inline cudaError_t enqueue_csr_build(cudaStream_t st, int64_t ntask, const int *
     int bits = 1;
     while (bits < 31 && ((int64_t)1 << bits) <= (int64_t)nleaf) ++bits;
     const int rtiles = (int)((ntask + kRadixTile - 1) / kRadixTile);
-    // (the 10-bit histogram of more than 2^20 tiles would overflow int)
+    // (10-bit digits up to 2^20 tiles: 4 GB of histogram and 8 GB of offsets there)
     const int digit = (bits > 16 && bits <= 20 && rtiles <= (1 << 20)) ? 10 : 8;
     const int passes = (bits + digit - 1) / digit;
-    const int nh = (1 << digit) * rtiles;
-    const int hscan_tiles = (nh + kScanTile - 1) / kScanTile;
+    const int nchunks = (rtiles + kColTiles - 1) / kColTiles;
     int *kbuf[2] = {b.keys_a, b.keys_b};
     int *vbuf[2] = {b.row_src, b.vals_b};
     const int *kin = nullptr, *vin = nullptr;
@@ -74,21 +77,45 @@ inline cudaError_t enqueue_csr_build(cudaStream_t st, int64_t ntask, const int *
         const int o = (passes - 1 - pass) & 1;  // the last pass lands in row_src
         int *kout = pass == passes - 1 ? nullptr : kbuf[o];
         int *vout = vbuf[o];
-        if (digit == 10)
-            radix_hist_kernel<10><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask, shift,
-                                                                       b.hist, rtiles);
-        else
-            radix_hist_kernel<8><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask, shift,
-                                                                      b.hist, rtiles);
-        scan_tiles_kernel<<<hscan_tiles, kScanThreads, 0, st>>>(b.hist, nh, b.hoffs, b.hsums);
-        scan_sums_kernel<<<1, kScanThreads, 0, st>>>(b.hsums, hscan_tiles, b.hoffs + nh);
-        scan_add_kernel<<<csr_grid(nh, 256, 1 << 30), 256, 0, st>>>(b.hoffs, nh, b.hsums);
-        if (digit == 10)
-            radix_scatter_kernel<10><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, vin, d_t, d_s, nleaf, ntask, shift,
-                                                                          b.hoffs, rtiles, kout, vout);
-        else
-            radix_scatter_kernel<8><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, vin, d_t, d_s, nleaf, ntask, shift,
-                                                                         b.hoffs, rtiles, kout, vout);
+        if (digit == 10) {
+            if (pass == 0)
+                radix_hist_kernel<10, true><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask,
+                                                                                 shift, b.hist, rtiles);
+            else
+                radix_hist_kernel<10, false><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask,
+                                                                                  shift, b.hist, rtiles);
+        } else {
+            if (pass == 0)
+                radix_hist_kernel<8, true><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask,
+                                                                                shift, b.hist, rtiles);
+            else
+                radix_hist_kernel<8, false><<<rtiles, kRadixWarps * 32, 0, st>>>(kin, d_t, d_s, nleaf, ntask,
+                                                                                 shift, b.hist, rtiles);
+        }
+        if (digit == 10) {
+            radix_colsum_kernel<1024><<<nchunks, 1024, 0, st>>>(b.hist, rtiles, b.hsums);
+            radix_colscan_kernel<1024><<<1, 1024, 0, st>>>(b.hsums, nchunks);
+            radix_offs_kernel<1024><<<nchunks, 1024, 0, st>>>(b.hist, rtiles, b.hsums, b.hoffs);
+        } else {
+            radix_colsum_kernel<256><<<nchunks, 256, 0, st>>>(b.hist, rtiles, b.hsums);
+            radix_colscan_kernel<256><<<1, 256, 0, st>>>(b.hsums, nchunks);
+            radix_offs_kernel<256><<<nchunks, 256, 0, st>>>(b.hist, rtiles, b.hsums, b.hoffs);
+        }
+        if (digit == 10) {
+            if (pass == 0)
+                radix_scatter_kernel<10, true><<<rtiles, kRadixWarps * 32, 0, st>>>(
+                    kin, vin, d_t, d_s, nleaf, ntask, shift, b.hoffs, rtiles, kout, vout);
+            else
+                radix_scatter_kernel<10, false><<<rtiles, kRadixWarps * 32, 0, st>>>(
+                    kin, vin, d_t, d_s, nleaf, ntask, shift, b.hoffs, rtiles, kout, vout);
+        } else {
+            if (pass == 0)
+                radix_scatter_kernel<8, true><<<rtiles, kRadixWarps * 32, 0, st>>>(
+                    kin, vin, d_t, d_s, nleaf, ntask, shift, b.hoffs, rtiles, kout, vout);
+            else
+                radix_scatter_kernel<8, false><<<rtiles, kRadixWarps * 32, 0, st>>>(
+                    kin, vin, d_t, d_s, nleaf, ntask, shift, b.hoffs, rtiles, kout, vout);
+        }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         *launches += 5;
         kin = kout;

@@ -245,31 +245,38 @@ csr_sort_rows_global_kernel(const int64_t *__restrict__ row_off, int nleaf, int 
     }
 }
 
-// Stable LSD radix sort of the list by sink id (8-bit digits), the CSR build:
-// within a row, entries keep list order - the order the reference's stable
-// thrust::sort_by_key gives (src/gpu_entry.cu:132) - so the pair kernels sum
-// every row in a fixed order and results repeat bit for bit.
+// Stable LSD radix sort of the list by sink id (8- or 10-bit digits), the CSR
+// build: within a row, entries keep list order - the order the reference's
+// stable thrust::sort_by_key gives (src/gpu_entry.cu:132) - so the pair
+// kernels sum every row in a fixed order and results repeat bit for bit.
 //
-// Per digit pass: radix_hist_kernel (per-tile 256-bin histogram, bin-major
-// so an exclusive scan gives every (bin, tile) its output offset), the scan,
-// radix_scatter_kernel (stable rank of each entry within its tile by digit,
-// from warp-private counts and __match_any_sync, then the scatter). Entries
-// with an out-of-range sink or source get key nleaf and sort past the rows.
+// Per digit pass: radix_hist_kernel (per-tile histogram, stored tile-major:
+// row t holds tile t's counts), the output offset of every (tile, digit) -
+// the digit's start plus the counts of that digit in earlier tiles - from a
+// column scan of the histogram (radix_colsum_kernel, radix_colscan_kernel,
+// radix_offs_kernel; every access a whole row), and radix_scatter_kernel: the
+// stable rank of each entry within its tile by digit (warp-private counts and
+// __match_any_sync), the tile reordered by digit in shared memory, then
+// written out so consecutive threads store consecutive entries of a digit's
+// run (a few sectors per warp store instead of one per entry). Entries with
+// an out-of-range sink or source get key nleaf and sort past the rows.
 constexpr int kRadixBins = 1024;  // most bins of a digit (10 bits); histograms are sized for it
 constexpr int kRadixWarps = 8;
 constexpr int kRadixRounds = 16;
 constexpr int kRadixTile = kRadixWarps * kRadixRounds * 32;  // 4096 entries
 
+// RAW (first pass): the key comes from the raw (t, s) list, else from keys.
+template <bool RAW>
 __device__ __forceinline__ unsigned radix_key(const int *keys, const int *raw_t, const int *raw_s,
                                               int nleaf, int64_t i) {
-    if (keys) return (unsigned)keys[i];
+    if (!RAW) return (unsigned)keys[i];
     const int t = raw_t[i], s = raw_s[i];
     return ((unsigned)t < (unsigned)nleaf && (unsigned)s < (unsigned)nleaf) ? (unsigned)t : (unsigned)nleaf;
 }
 
-// keys == nullptr: first pass, keys computed from the raw (t, s) list.
+// RAW: first pass, keys computed from the raw (t, s) list (keys unused).
 // BITS: digit width (8 or 10).
-template <int BITS>
+template <int BITS, bool RAW>
 __global__ void __launch_bounds__(kRadixWarps * 32)
 radix_hist_kernel(const int *__restrict__ keys, const int *__restrict__ raw_t,
                   const int *__restrict__ raw_s, int nleaf, int64_t n, int shift,
@@ -281,21 +288,26 @@ radix_hist_kernel(const int *__restrict__ keys, const int *__restrict__ raw_t,
     for (int b = threadIdx.x; b < kRadixWarps * NB; b += blockDim.x) (&h[0][0])[b] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * kRadixTile + (int64_t)w * kRadixRounds * 32;
-#pragma unroll 4
+    // all rounds' loads first (in flight together), then the counts
+    unsigned key[kRadixRounds];
+#pragma unroll
     for (int r = 0; r < kRadixRounds; ++r) {
         const int64_t i = base + r * 32 + lane;
-        if (i < n) atomicAdd(&h[w][(radix_key(keys, raw_t, raw_s, nleaf, i) >> shift) & MASK], 1);
+        key[r] = i < n ? radix_key<RAW>(keys, raw_t, raw_s, nleaf, i) : 0xffffffffu;
     }
+#pragma unroll
+    for (int r = 0; r < kRadixRounds; ++r)
+        if (key[r] != 0xffffffffu) atomicAdd(&h[w][(key[r] >> shift) & MASK], 1);
     __syncthreads();
     for (int b = threadIdx.x; b < NB; b += blockDim.x) {
         int tot = 0;
 #pragma unroll
         for (int q = 0; q < kRadixWarps; ++q) tot += h[q][b];
-        hist[(int64_t)b * ntiles + blockIdx.x] = tot;
+        hist[(int64_t)blockIdx.x * NB + b] = tot;
     }
 }
 
-template <int BITS>
+template <int BITS, bool RAW>
 __global__ void __launch_bounds__(kRadixWarps * 32)
 radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
                      const int *__restrict__ raw_t, const int *__restrict__ raw_s, int nleaf,
@@ -303,32 +315,55 @@ radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
                      int *__restrict__ keys_out, int *__restrict__ vals_out) {
     constexpr int NB = 1 << BITS;
     constexpr unsigned MASK = NB - 1u;
-    __shared__ int cnt[kRadixWarps][NB];
-    __shared__ int64_t gbase[NB];
+    constexpr int NT = kRadixWarps * 32;
+    constexpr int BPT = NB / NT;  // bins per thread in the bin scans
+    static_assert(NB % NT == 0, "bins must split evenly over the block");
+    constexpr int POOL = kRadixWarps * NB > 2 * kRadixTile ? kRadixWarps * NB : 2 * kRadixTile;
+    // the warp counts (warp q, digit b at pool[q * NB + b]), then, once every
+    // entry's tile position is known, the tile's keys and values in digit order
+    __shared__ int pool[POOL];
+    __shared__ int bin_start[NB];      // exclusive start of each digit within the tile
+    __shared__ int64_t gdelta[NB];     // output offset of the digit's run minus its start in the tile
+    __shared__ int wsum[kRadixWarps];
+    int(*cnt)[NB] = reinterpret_cast<int(*)[NB]>(pool);
+    int *tkeys = pool;
+    int *tvals = pool + kRadixTile;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    for (int b = threadIdx.x; b < kRadixWarps * NB; b += blockDim.x) (&cnt[0][0])[b] = 0;
-    for (int b = threadIdx.x; b < NB; b += blockDim.x)
-        gbase[b] = offs[(int64_t)b * ntiles + blockIdx.x];
-    __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * kRadixTile + (int64_t)w * kRadixRounds * 32;
+    int64_t goff[BPT];  // this thread's digits' output offsets, loaded early
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) goff[k] = offs[(int64_t)blockIdx.x * NB + threadIdx.x * BPT + k];
+    const int64_t tile0 = (int64_t)blockIdx.x * kRadixTile;
+    const int64_t base = tile0 + (int64_t)w * kRadixRounds * 32;
     unsigned key[kRadixRounds];
     int val[kRadixRounds];
     unsigned peers[kRadixRounds];
+    // all rounds' loads first (in flight together), then the ranks
 #pragma unroll
     for (int r = 0; r < kRadixRounds; ++r) {
         const int64_t i = base + r * 32 + lane;
         const bool ok = i < n;
-        key[r] = ok ? radix_key(keys, raw_t, raw_s, nleaf, i) : 0xffffffffu;
-        val[r] = ok ? (vals ? vals[i] : raw_s[i]) : 0;
+        key[r] = ok ? radix_key<RAW>(keys, raw_t, raw_s, nleaf, i) : 0xffffffffu;
+        val[r] = ok ? (RAW ? raw_s[i] : vals[i]) : 0;
+    }
+    for (int b = threadIdx.x; b < kRadixWarps * NB; b += NT) pool[b] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRadixRounds; ++r) {
+        const bool ok = base + r * 32 + lane < n;
         const int d = ok ? (int)((key[r] >> shift) & MASK) : NB + lane;  // tail lanes: own group
         peers[r] = __match_any_sync(kFull, d);
         if (ok && lane == __ffs(peers[r]) - 1) cnt[w][d] += __popc(peers[r]);
         __syncwarp();
     }
     __syncthreads();
-    // exclusive base of every warp within the tile, per bin
-    for (int b = threadIdx.x; b < NB; b += blockDim.x) {
+    // per digit: exclusive base of every warp within the digit's run, the
+    // run's length, then the runs' starts (a block scan over the digits)
+    int tot[BPT];
+    int run_sum = 0;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int b = threadIdx.x * BPT + k;
         int run = 0;
 #pragma unroll
         for (int q = 0; q < kRadixWarps; ++q) {
@@ -336,22 +371,130 @@ radix_scatter_kernel(const int *__restrict__ keys, const int *__restrict__ vals,
             cnt[q][b] = run;
             run += c;
         }
+        tot[k] = run;
+        run_sum += run;
+    }
+    int incl = run_sum;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, off);
+        if (lane >= off) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    int start = incl - run_sum;
+    for (int q = 0; q < w; ++q) start += wsum[q];
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int b = threadIdx.x * BPT + k;
+        bin_start[b] = start;
+        gdelta[b] = goff[k] - start;
+        start += tot[k];
     }
     __syncthreads();
+    // each entry's position within the tile (digit order, list order within a digit)
+    int lp[kRadixRounds];
 #pragma unroll
     for (int r = 0; r < kRadixRounds; ++r) {
-        const int64_t i = base + r * 32 + lane;
-        const bool ok = i < n;
+        const bool ok = base + r * 32 + lane < n;
         const int d = ok ? (int)((key[r] >> shift) & MASK) : 0;
         const int before = ok ? cnt[w][d] : 0;
         __syncwarp();
-        if (ok) {
-            const int64_t pos = gbase[d] + before + __popc(peers[r] & lt);
-            if (keys_out) keys_out[pos] = (int)key[r];
-            vals_out[pos] = val[r];
-            if (lane == __ffs(peers[r]) - 1) cnt[w][d] = before + __popc(peers[r]);
-        }
+        lp[r] = ok ? bin_start[d] + before + __popc(peers[r] & lt) : -1;
+        if (ok && lane == __ffs(peers[r]) - 1) cnt[w][d] = before + __popc(peers[r]);
         __syncwarp();
+    }
+    __syncthreads();  // the warp counts are dead: the tile is staged over them
+#pragma unroll
+    for (int r = 0; r < kRadixRounds; ++r) {
+        if (lp[r] >= 0) {
+            tkeys[lp[r]] = (int)key[r];
+            tvals[lp[r]] = val[r];
+        }
+    }
+    __syncthreads();
+    // consecutive threads write consecutive entries of a digit's run
+    const int tn = (int)min((int64_t)kRadixTile, n - tile0);
+    for (int j = threadIdx.x; j < tn; j += NT) {
+        const unsigned k = (unsigned)tkeys[j];
+        const int64_t pos = gdelta[(k >> shift) & MASK] + j;
+        if (keys_out) keys_out[pos] = (int)k;
+        vals_out[pos] = tvals[j];
+    }
+}
+
+// Column scan of the tile-major histogram in chunks of kColTiles tiles:
+// csum[c * NB + d] = count of digit d in chunk c (radix_colsum_kernel), then
+// in place the exclusive prefix over chunks plus digit d's start in the
+// output (radix_colscan_kernel, one block), then offs[t * NB + d], tile t's
+// output offset for digit d (radix_offs_kernel). One thread per digit; the
+// threads of a block read and write whole rows.
+constexpr int kColTiles = 128;
+
+template <int NB>
+__global__ void __launch_bounds__(NB)
+radix_colsum_kernel(const int *__restrict__ hist, int ntiles, int64_t *__restrict__ csum) {
+    const int d = threadIdx.x;
+    const int t0 = blockIdx.x * kColTiles, t1 = min(ntiles, t0 + kColTiles);
+    int64_t s = 0;
+#pragma unroll 8
+    for (int t = t0; t < t1; ++t) s += hist[(int64_t)t * NB + d];
+    csum[(int64_t)blockIdx.x * NB + d] = s;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(NB)
+radix_colscan_kernel(int64_t *__restrict__ csum, int nchunks) {
+    constexpr int NW = NB / 32;
+    __shared__ int64_t wsum[NW];
+    const int d = threadIdx.x, lane = d & 31, w = d >> 5;
+    int64_t tot = 0;
+#pragma unroll 8
+    for (int c = 0; c < nchunks; ++c) tot += csum[(int64_t)c * NB + d];
+    // digit starts: exclusive scan of the totals over the digits
+    int64_t x = tot;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int64_t y = __shfl_up_sync(kFull, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t v = lane < NW ? wsum[lane] : 0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int64_t y = __shfl_up_sync(kFull, v, off);
+            if (lane >= off) v += y;
+        }
+        if (lane < NW) wsum[lane] = v;
+    }
+    __syncthreads();
+    int64_t run = x - tot + (w > 0 ? wsum[w - 1] : 0);
+    for (int c = 0; c < nchunks; ++c) {
+        const int64_t i = (int64_t)c * NB + d;
+        const int64_t v = csum[i];
+        csum[i] = run;
+        run += v;
+    }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(NB)
+radix_offs_kernel(const int *__restrict__ hist, int ntiles, const int64_t *__restrict__ csum,
+                  int64_t *__restrict__ offs) {
+    const int d = threadIdx.x;
+    const int t0 = blockIdx.x * kColTiles, t1 = min(ntiles, t0 + kColTiles);
+    int64_t run = csum[(int64_t)blockIdx.x * NB + d];
+    for (int k0 = t0; k0 < t1; k0 += 8) {
+        int h[8];  // eight rows' loads in flight
+#pragma unroll
+        for (int k = 0; k < 8; ++k) h[k] = k0 + k < t1 ? hist[(int64_t)(k0 + k) * NB + d] : 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (k0 + k < t1) offs[(int64_t)(k0 + k) * NB + d] = run;
+            run += h[k];
+        }
     }
 }
 
