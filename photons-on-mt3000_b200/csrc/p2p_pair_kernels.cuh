@@ -392,7 +392,7 @@ struct SinkPair {
 
 // Tuning knobs of the packed kernel (compile time).
 #ifndef P2P_X2_GROUP
-#define P2P_X2_GROUP 4  // packed sink pairs per predicated block (8 sinks)
+#define P2P_X2_GROUP 4  // packed sink pairs per predicated block in the first half of the tile (8 sinks)
 #endif
 #ifndef P2P_X2_MINBLOCKS
 #define P2P_X2_MINBLOCKS 3  // resident 128-thread blocks per SM the register budget targets
@@ -403,7 +403,11 @@ struct SinkPair {
 #ifndef P2P_X2_SINKPAIRS
 #define P2P_X2_SINKPAIRS 16  // sink pairs per slice (a slice holds 2x that many sinks)
 #endif
+#ifndef P2P_X2_TAILGROUP
+#define P2P_X2_TAILGROUP 2  // packed sink pairs per predicated block in the second half of the tile
+#endif
 constexpr int kPairGroup = P2P_X2_GROUP;
+constexpr int kTailGroup = P2P_X2_TAILGROUP;
 
 // H(t) for two sinks at once: Horner's rule, one packed FMA per coefficient.
 // (Measured alternatives: two scalar Horner chains, Estrin's scheme,
@@ -621,27 +625,30 @@ pair_split_src2_kernel(const __grid_constant__ PairArgs a, const int stage_cap) 
                     // cutoff skip the select and the band test
                     const bool check = __any_sync(kFull, slot >= fill || sidx[slot] < 0);
                     bool amb = false;
+                    // sink pairs in blocks of kPairGroup over the first half
+                    // of the tile and of kTailGroup over the second, where the
+                    // last, partly filled block usually falls (less padding)
+#define P2P_X2_SWEEP(CHK)                                                                                     \
+    _Pragma("unroll") for (int g = 0; g < NP / 2; g += kPairGroup) {                                         \
+        if (2 * g < ns) {                                                                                    \
+            _Pragma("unroll") for (int q = 0; q < kPairGroup; ++q)                                           \
+                pair_split_x2<SOFT, MASSES, NC, CHK>(sx, sy, sz, src.w, sinks[g + q], a, eps2v, negu0v,       \
+                                                     ax[g + q], ay[g + q], az[g + q], amb);                  \
+        }                                                                                                    \
+    }                                                                                                        \
+    _Pragma("unroll") for (int g = NP / 2; g < NP; g += kTailGroup) {                                        \
+        if (2 * g < ns) {                                                                                    \
+            _Pragma("unroll") for (int q = 0; q < kTailGroup; ++q)                                           \
+                pair_split_x2<SOFT, MASSES, NC, CHK>(sx, sy, sz, src.w, sinks[g + q], a, eps2v, negu0v,       \
+                                                     ax[g + q], ay[g + q], az[g + q], amb);                  \
+        }                                                                                                    \
+    }
                     if (check) {
-#pragma unroll
-                        for (int g = 0; g < NP; g += kPairGroup) {
-                            if (2 * g < ns) {
-#pragma unroll
-                                for (int q = 0; q < kPairGroup; ++q)
-                                    pair_split_x2<SOFT, MASSES, NC, true>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                          negu0v, ax[g + q], ay[g + q], az[g + q], amb);
-                            }
-                        }
+                        P2P_X2_SWEEP(true)
                     } else {
-#pragma unroll
-                        for (int g = 0; g < NP; g += kPairGroup) {
-                            if (2 * g < ns) {
-#pragma unroll
-                                for (int q = 0; q < kPairGroup; ++q)
-                                    pair_split_x2<SOFT, MASSES, NC, false>(sx, sy, sz, src.w, sinks[g + q], a, eps2v,
-                                                                           negu0v, ax[g + q], ay[g + q], az[g + q], amb);
-                            }
-                        }
+                        P2P_X2_SWEEP(false)
                     }
+#undef P2P_X2_SWEEP
                     ambmask |= amb ? (1u << ci) : 0u;
                 }
                 // rare: pairs within the cutoff band, decided in FP64
