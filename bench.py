@@ -139,6 +139,19 @@ def load_traffic(workload, form_name):
         return None
 
 
+def load_fp64_flops(workload):
+    """FP64 flops per listed pair of the plain form's pair kernel (DFMA x 2 +
+    DADD + DMUL per pair, CUDA's erfc/exp/rsqrt included) from the committed
+    ncu summary, or None."""
+    path = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(f"{workload}:plain_fp64:fp64_flops_per_pair")
+    except (OSError, ValueError):
+        return None
+
+
 def combine_ranks(total_s, e2e_s, pairs, dist, device):
     """Whole-job figures of a replica run: the slowest rank's times (max over
     ranks) and the pair interactions of all ranks (sum)."""
@@ -151,6 +164,22 @@ def combine_ranks(total_s, e2e_s, pairs, dist, device):
     pt = torch.tensor([float(pairs)], dtype=torch.float64, device=device)
     dist.all_reduce(pt, op=dist.ReduceOp.SUM)
     return float(t[0]), float(t[1]), float(pt[0])
+
+
+def plain_roofline(workload, pairs, kernel_ms, fp64_peak, fp32_peak):
+    """The plain FP64 form's pair kernel against the measured FP64 and FP32
+    peaks: FP64 flops per pair counted by ncu (the form's own arithmetic
+    calls CUDA's FP64 erfc, exp and rsqrt, so its flops are counted where they
+    execute rather than from the source)."""
+    f64 = load_fp64_flops(workload)
+    if not f64:
+        return {"bound": "fp64", "peak": fp64_peak, "unit": "TFLOP/s", "flops_per_pair": None}
+    achieved = pairs / (kernel_ms * 1e-3) * f64 / 1e12
+    return {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": achieved / fp64_peak, "frac_of_fp32_peak": achieved / fp32_peak,
+            "fp32_peak": fp32_peak, "flops_per_pair": f64,
+            "flops_source": "ncu: 2 DFMA + DADD + DMUL per listed pair (128^3 capture)",
+            "peak_source": "DFMA chain microbenchmark in-process (measured)"}
 
 
 def run_ours(args, rank, world, dist):
@@ -210,6 +239,7 @@ def run_ours(args, rank, world, dist):
 
     with Session(local) as sess:
         fp32_peak = sess.measure_fp32_peak()
+        fp64_peak = sess.measure_fp64_peak()
         sess.set_params(params_for(cfg, form, mass))
         degree = sess.poly_degree
         sampler = ClockSampler(local)
@@ -224,6 +254,7 @@ def run_ours(args, rank, world, dist):
             sess.set_params(params_for(cfg, abi.FORM_PLAIN_FP64, mass))
             p_s, p_k, _ = resident_passes(sess, max(1, min(args.steps, 3)), 1)
             plain = {"value": P / float(np.mean(p_s)), "kernel_ms": float(np.mean(p_k))}
+            plain["roofline"] = plain_roofline(args.workload, P, plain["kernel_ms"], fp64_peak, fp32_peak)
             loc = tl.tag == 1
             acc_plain = result(sess)
             num = np.linalg.norm(acc_form - acc_plain, axis=0)[loc]
@@ -268,6 +299,8 @@ def run_ours(args, rank, world, dist):
     F = flops_per_pair(cfg.soft_mode, degree) if form != abi.FORM_PLAIN_FP64 else None
     kernel_pairs_per_s = P / (mean_kernel_ms * 1e-3)
     roofline = None
+    if form == abi.FORM_PLAIN_FP64:
+        roofline = plain_roofline(args.workload, P, mean_kernel_ms, fp64_peak, fp32_peak)
     if F:
         # flops of the pairs the kernel evaluates (entries wholly beyond the
         # cutoff are skipped: counted in the metric's pairs, not in the flops)

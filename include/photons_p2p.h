@@ -196,6 +196,10 @@ int p2p_pass_noalloc(const p2p_params *params, int npart, const double *d_pos, i
  * dependent-chain microbenchmark run on the session stream. */
 int p2p_measure_fp32_peak(p2p_session *s, double *tflops);
 
+/* Measured FP64 DFMA throughput of this GPU (TFLOP/s, FMA = 2 flops), the
+ * same microbenchmark in double precision. */
+int p2p_measure_fp64_peak(p2p_session *s, double *tflops);
+
 /* ---- Serving an ensemble of boxes (no counterpart in the reference) -----
  * A server takes force-pass requests for many independent periodic boxes.
  * Each box's particles, leaf frames and CSR list are built once on the

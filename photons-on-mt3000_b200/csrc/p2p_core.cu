@@ -796,3 +796,27 @@ P2P_API int p2p_measure_fp32_peak(p2p_session *s, double *tflops) {
     s->kernel_timed = false;
     return P2P_OK;
 }
+
+P2P_API int p2p_measure_fp64_peak(p2p_session *s, double *tflops) {
+    P2P_TRY(check_session(s));
+    if (!tflops) return fail(P2P_ERR_ARG, "null argument");
+    const int threads = 256, blocks = s->sm_count * 8, iters = 1024;
+    P2P_TRY(ensure(s, s->probe, sizeof(double) * (size_t)threads * blocks));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        CUDA_TRY(cudaEventRecord(s->ev_k0, s->stream));
+        dfma_probe_kernel<<<blocks, threads, 0, s->stream>>>((double *)s->probe.p, iters, 0.9999999999,
+                                                             1e-12);
+        CUDA_TRY(cudaGetLastError());
+        launch_count(1);
+        CUDA_TRY(cudaEventRecord(s->ev_k1, s->stream));
+        CUDA_TRY(cudaEventSynchronize(s->ev_k1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, s->ev_k0, s->ev_k1));
+        best = std::min(best, ms);
+    }
+    const double flops = 2.0 * 8 * 8 * (double)iters * threads * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    s->kernel_timed = false;
+    return P2P_OK;
+}

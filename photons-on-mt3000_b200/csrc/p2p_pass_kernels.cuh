@@ -592,4 +592,19 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float *out, int iters, f
     if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// FP64 DFMA throughput: the same chains in double precision.
+__global__ void __launch_bounds__(256) dfma_probe_kernel(double *out, int iters, double m, double b) {
+    double x0 = threadIdx.x * 1e-7, x1 = x0 + 1.0, x2 = x0 + 2.0, x3 = x0 + 3.0;
+    double x4 = x0 + 4.0, x5 = x0 + 5.0, x6 = x0 + 6.0, x7 = x0 + 7.0;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            x0 = fma(x0, m, b); x1 = fma(x1, m, b); x2 = fma(x2, m, b); x3 = fma(x3, m, b);
+            x4 = fma(x4, m, b); x5 = fma(x5, m, b); x6 = fma(x6, m, b); x7 = fma(x7, m, b);
+        }
+    }
+    const double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1234.5) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace p2p

@@ -112,6 +112,7 @@ SIGNATURES = {
     "p2p_kernel_launch_count": (_i64, []),
     "p2p_session_last_kernel_ms": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
     "p2p_measure_fp32_peak": (_i, [_vp, ctypes.POINTER(_d)]),
+    "p2p_measure_fp64_peak": (_i, [_vp, ctypes.POINTER(_d)]),
     "p2p_pass_noalloc": (_i, [ctypes.POINTER(Params), _i, _vp, _i, _vp, _vp, _i64, _vp, _vp, _vp, _vp]),
     "p2p_server_config_default": (None, [ctypes.POINTER(ServerConfig)]),
     "p2p_server_create": (_i, [_i, ctypes.POINTER(Params), ctypes.POINTER(ServerConfig),

@@ -160,6 +160,11 @@ class Session:
         _check(self.lib, self.lib.p2p_measure_fp32_peak(self.h, ctypes.byref(v)))
         return v.value
 
+    def measure_fp64_peak(self):
+        v = ctypes.c_double()
+        _check(self.lib, self.lib.p2p_measure_fp64_peak(self.h, ctypes.byref(v)))
+        return v.value
+
 
 def kernel_launch_count():
     return _native.core().p2p_kernel_launch_count()

@@ -332,3 +332,15 @@ def test_plain_matches_oracle_with_ten_bit_radix(gpu):
         sinks[tl.leaf_ipart[l]:tl.leaf_ipart[l] + tl.leaf_npart[l]] = True
     rms, mx = rel_err(got, ref, sinks)
     assert mx <= PLAIN_MAX, mx
+
+
+def test_throughput_probes(gpu):
+    """The FP32 and FP64 throughput probes whose results are the rooflines'
+    peaks: positive, below the B200's nominal figures at 1965 MHz (74.4 FP32,
+    37.2 FP64 TFLOP/s) with margin, FP64 slower than FP32."""
+    with Session(gpu) as s:
+        f32 = s.measure_fp32_peak()
+        f64 = s.measure_fp64_peak()
+    assert 10.0 < f32 < 80.0, f32
+    assert 5.0 < f64 < 42.0, f64
+    assert f64 < f32
