@@ -77,7 +77,7 @@ def build_workload(name, rank=0):
         g = W.rng(1000 + rank)
         pos = np.mod(pos + g.random((3, 1)), 1.0) * cfg.box + cfg.origin
     tl = W.prepare(pos, cfg)
-    return cfg, pos.shape[1], tl
+    return cfg, pos.shape[1], tl, pos
 
 
 class ClockSampler:
@@ -182,6 +182,49 @@ def plain_roofline(workload, pairs, kernel_ms, fp64_peak, fp32_peak):
             "peak_source": "DFMA chain microbenchmark in-process (measured)"}
 
 
+def walk_leg(sess, cfg, raw_pos, tl, dev, d_pos, d_ip, d_np, pairs, steps=3):
+    """The P2P lists walked on the GPU (p2p_pass_submit_walk) against the
+    caller's serial walk on the host cores: the host walk's time, and whole
+    passes (frame prep, device walk, pair kernel) on resident particles."""
+    from photons_p2p import lists as L
+    from photons_p2p.p2p import DeviceWalkTree, kernel_launch_count
+
+    allpos, tag = W.with_ghosts(raw_pos, cfg)
+    t0 = time.time()
+    tree = L.Tree(allpos, tag, cfg.maxleaf, cfg.box)
+    tree_s = time.time() - t0
+    with tree:
+        if not (np.array_equal(tree.leaf_ipart, tl.leaf_ipart) and np.array_equal(tree.perm, tl.perm)):
+            raise RuntimeError("walk leg: the tree differs from the pass's tree")
+        t0 = time.time()
+        tt, _ = tree.walk(cfg.cutoff_radius, cfg.open_angle)
+        host_walk_s = time.time() - t0
+        ntask_host = len(tt)
+        del tt
+        dtree = DeviceWalkTree(tree, dev)
+        lib = sess.lib
+        times, kern, ntask = [], [], 0
+        l0 = kernel_launch_count()
+        for k in range(steps + 1):
+            if lib.p2p_pass_begin_device(sess.h, tl.npart, d_pos.data_ptr(), None, tl.nleaf, d_ip.data_ptr(),
+                                         d_np.data_ptr()):
+                raise RuntimeError(lib.p2p_last_error().decode())
+            ntask = sess.submit_walk(dtree, cfg.cutoff_radius, cfg.open_angle)
+            sec = sess.end()
+            if k:  # the first pass warms up
+                times.append(sec)
+                kern.append(sess.last_kernel_ms())
+        launches = (kernel_launch_count() - l0) // (steps + 1)
+        walk_pairs = sess.pair_count()
+    pass_s, kern_ms = float(np.mean(times)), float(np.mean(kern))
+    return {"host_tree_s": round(tree_s, 2), "host_walk_s": round(host_walk_s, 2),
+            "host_walk_cores": L.num_threads(), "entries": int(ntask),
+            "entries_equal_host": bool(ntask == ntask_host), "pairs_equal": bool(walk_pairs == pairs),
+            "pass_ms": 1e3 * pass_s, "pair_kernel_ms": kern_ms,
+            "walk_and_prep_ms": 1e3 * pass_s - kern_ms, "pairs_per_s": pairs / pass_s,
+            "gpu_launches_per_pass": int(launches)}
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -191,7 +234,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     t0 = time.time()
-    cfg, nlocal, tl = build_workload(args.workload, rank)
+    cfg, nlocal, tl, raw_pos = build_workload(args.workload, rank)
     prep_s = time.time() - t0
     mass = 1.0 / nlocal
     P = tl.pair_count()
@@ -289,6 +332,9 @@ def run_ours(args, rank, world, dist):
             e2e_t.append(time.perf_counter() - a)
         h2d = tl.pos.nbytes + tl.leaf_ipart.nbytes + tl.leaf_npart.nbytes + tl.task_t.nbytes + tl.task_s.nbytes
         d2h = 3 * tl.npart * 8
+        walk = None
+        if not args.no_walk:
+            walk = walk_leg(sess, cfg, raw_pos, tl, dev, d_pos, d_ip, d_np, P)
 
     mean_pass = float(np.mean(pass_s))
     mean_kernel_ms = float(np.mean(kern_ms))
@@ -328,6 +374,7 @@ def run_ours(args, rank, world, dist):
         "roofline": roofline,
         "plain_fp64": plain,
         "split_over_plain": (value / plain["value"]) if plain else None,
+        "device_walk": walk,
         "accuracy": accuracy,
         "e2e": {"value": P_all / e2e_mean, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -611,6 +658,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary")
+    ap.add_argument("--no-walk", action="store_true", help="skip the device list walk leg")
     ap.add_argument("--boxes", type=int, default=512, help="c4: ensemble size")
     ap.add_argument("--slots", type=int, default=1, help="c4: server launch slots")
     ap.add_argument("--hbm-gb", type=float, default=100.0, help="c4: server arena size")
@@ -639,7 +687,7 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             t0 = time.time()
-            cfg, nlocal, tl = build_workload(args.workload, 0)
+            cfg, nlocal, tl, _ = build_workload(args.workload, 0)
             mass = 1.0 / nlocal
             if args.warmup:
                 time_cpu(cfg, tl, mass, min(args.cpu_pairs, 2e8))

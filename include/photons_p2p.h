@@ -150,6 +150,37 @@ int p2p_pass_run_device(p2p_session *s, int npart, const double *d_pos, const do
                         int nleaf, const int *d_leaf_ipart, const int *d_leaf_npart,
                         int64_t ntask, const int *d_task_t, const int *d_task_s);
 
+/* ---- Device list walk (no counterpart in the reference's GPU code) ------
+ * The caller's kd-tree, as PhotoNs builds it (build_kdtree / center_kdtree,
+ * src/fmm.c:231-327), in device memory; child codes are leaf l -> 2l and
+ * node k -> 2k+1, the root is node 0, leaves are numbered in pre-order (the
+ * leaves of son[0]'s subtree precede those of son[1]'s). */
+typedef struct p2p_walk_tree {
+    int nnode, nleaf;
+    const int *son;             /* 2*nnode child codes */
+    const int *node_first;      /* nnode: smallest leaf id in the node's subtree */
+    const double *node_center;  /* 3*nnode (AoS) box centres, src/fmm.c:273-327 */
+    const double *node_width;   /* 3*nnode box widths */
+    const double *leaf_center;  /* 3*nleaf */
+    const double *leaf_width;   /* 3*nleaf */
+    const int *leaf_active;     /* nleaf: >= 0 for leaves with a local particle (sinks) */
+} p2p_walk_tree;
+/* Replaces the caller's walk_task_p2p (src/fmm.c:656-792, acceptance
+ * src/fmm.c:409-479, called from fmm_task src/fmm.c:1221-1300) plus the
+ * list submit: the P2P lists are walked on the GPU, one thread per sink leaf,
+ * straight into CSR rows equal entry for entry to those p2p_pass_submit
+ * builds from the serial walk's list, then the pair kernel runs on them.
+ * Within an open pass (its leaves are the tree's leaves). Waits for the row
+ * count (one device-to-host read); *ntask (nullable) = list entries.
+ * P2P_ERR_ARG for a child code outside the tree, P2P_ERR_CAPACITY when a
+ * sink's pending pairs exceed the walk's fixed stack. */
+int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *tree, double cutoff, double open_angle,
+                         int64_t *ntask);
+/* Host copy of the CSR rows of the last submitted chunk or walk (row_off:
+ * nleaf+1 entries; row_src (nullable: rows not copied): row_off[nleaf]
+ * entries). Call after p2p_pass_end. */
+int p2p_pass_rows(p2p_session *s, int64_t *row_off, int *row_src);
+
 /* Waits for all work queued on the session stream. */
 int p2p_session_synchronize(p2p_session *s);
 

@@ -22,7 +22,7 @@ CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu", "p2p_pair_sink_lanes.cu", "p2p_
                 "p2p_pair_source_lanes_x2_f32.cu", "p2p_pair_plain.cu", "p2p_server.cu", "p2p_pair_sink_lanes_x2.cu"]
 CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_pass_kernels.cuh", "p2p_pair_kernels.cuh",
                 "p2p_device_common.cuh", "p2p_launch.h", "p2p_internal.h", "p2p_fit.h",
-                "p2p_pair_x2_impl.h", "p2p_csr.h", "p2p_args.h", "p2p_host_shared.h"]
+                "p2p_pair_x2_impl.h", "p2p_csr.h", "p2p_args.h", "p2p_host_shared.h", "p2p_walk_kernels.cuh"]
 HOST_SOURCES = ["p2p_lists.cpp"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -44,7 +44,7 @@ def build_lists(force=False):
     target = os.path.join(OUT, "libphotons_lists.so")
     srcs = [os.path.join(HERE, "host", s) for s in HOST_SOURCES]
     if force or _stale(target, srcs + [__file__]):
-        _run(["g++", "-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-fopenmp", "-shared",
+        _run(["g++", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-std=c++17", "-fPIC", "-fopenmp", "-shared",
               "-o", target] + srcs)
     return target
 

@@ -20,6 +20,7 @@
 #include "p2p_launch.h"
 #include "p2p_host_shared.h"
 #include "p2p_pass_kernels.cuh"
+#include "p2p_walk_kernels.cuh"
 
 namespace p2p {
 #include "p2p_csr.h"
@@ -297,6 +298,15 @@ int size_radix_buffers(p2p_session *s, int64_t ntask) {
     return P2P_OK;
 }
 
+int enqueue_pairs(p2p_session *s, bool timed);
+
+// Whether the pair kernel of these parameters skips entries wholly beyond the
+// cutoff (their pairs are then counted apart, for the evaluated-pair count).
+bool skips_outside(const p2p_session *s) {
+    return packed_lanes(s->params) ||
+           (is_fp32_form(s->params.form) && s->params.kernel_variant == P2P_VARIANT_SINK_LANES_X2);
+}
+
 // CSR build + pair kernel for one list chunk already on the device.
 int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed,
                   cudaEvent_t lists_read = nullptr) {
@@ -313,8 +323,7 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
     b.hoffs = (int64_t *)s->hoffs.p;
     b.hsums = (int64_t *)s->hsums.p;
     b.pairs = (unsigned long long *)s->pairs.p;
-    if (packed_lanes(s->params) ||
-        (is_fp32_form(s->params.form) && s->params.kernel_variant == P2P_VARIANT_SINK_LANES_X2)) {
+    if (skips_outside(s)) {
         // the packed kernels skip entries wholly beyond the cutoff; count their pairs
         b.skipped = (unsigned long long *)s->skipped.p;
         b.cscale = 0.5 / s->params.split_radius;
@@ -326,6 +335,11 @@ int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s,
                                &launched));
     launch_count(launched);
     if (lists_read) CUDA_TRY(cudaEventRecord(lists_read, s->stream));  // d_t / d_s may be reused
+    return enqueue_pairs(s, timed);
+}
+
+// The pair kernel over the session's CSR rows (row_off, row_src).
+int enqueue_pairs(p2p_session *s, bool timed) {
     CUDA_TRY(cudaMemsetAsync(s->queue.p, 0, sizeof(int), s->stream));
     PairArgs a = make_args(s);
     // Inside a stream capture the kernel's events become external event-record
@@ -641,6 +655,81 @@ P2P_API int p2p_pass_end(p2p_session *s, double *gpu_seconds) {
     CUDA_TRY(cudaMemcpy(&status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (status & ST_LEAF_RANGE) return fail(P2P_ERR_RANGE, "a leaf range lies outside the particles");
     if (status & ST_TASK_RANGE) return fail(P2P_ERR_RANGE, "a task entry names a leaf outside [0, nleaf)");
+    if (status & ST_WALK_TREE) return fail(P2P_ERR_ARG, "walk: a child code outside the tree");
+    if (status & (ST_WALK_STACK | ST_WALK_ROW)) return fail(P2P_ERR_CAPACITY, "walk: a sink's walk exceeded its stack");
+    return P2P_OK;
+}
+
+P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double cutoff, double open_angle,
+                                 int64_t *ntask) {
+    P2P_TRY(check_session(s));
+    if (!s->in_pass) return fail(P2P_ERR_STATE, "no open pass");
+    if (!t) return fail(P2P_ERR_ARG, "null tree");
+    if (t->nleaf != s->nleaf) return fail(P2P_ERR_ARG, "tree has %d leaves, the pass %d", t->nleaf, s->nleaf);
+    if (t->nnode < 0) return fail(P2P_ERR_ARG, "negative size");
+    if ((t->nnode > 0 && (!t->son || !t->node_first || !t->node_center || !t->node_width)) ||
+        (t->nleaf > 0 && (!t->leaf_center || !t->leaf_width || !t->leaf_active)))
+        return fail(P2P_ERR_ARG, "null tree array");
+    if (!(cutoff >= 0.0) || !(open_angle >= 0.0)) return fail(P2P_ERR_ARG, "bad cutoff or open angle");
+    if (ntask) *ntask = 0;
+    const int nleaf = s->nleaf;
+    if (nleaf == 0 || t->nnode == 0) return P2P_OK;
+    WalkArgs w;
+    w.nnode = t->nnode;
+    w.nleaf = nleaf;
+    w.son = t->son;
+    w.node_first = t->node_first;
+    w.leaf_active = t->leaf_active;
+    w.node_center = t->node_center;
+    w.node_width = t->node_width;
+    w.leaf_center = t->leaf_center;
+    w.leaf_width = t->leaf_width;
+    w.cutoff = cutoff;
+    w.open_angle = open_angle;
+    const int threads = 128;
+    const int grid = grid_for(nleaf, threads, s->sm_count * 64);
+    int *status = (int *)s->status.p;
+    // pass 1: row lengths, then the row offsets
+    walk_rows_kernel<false><<<grid, threads, 0, s->stream>>>(w, (int *)s->counts.p, nullptr, nullptr, nullptr,
+                                                               nullptr, 0.0, 0.f, nullptr, nullptr, status);
+    const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
+    int64_t *row_off = (int64_t *)s->row_off.p;
+    scan_tiles_kernel<<<ntiles, kScanThreads, 0, s->stream>>>((const int *)s->counts.p, nleaf, row_off,
+                                                               (int64_t *)s->tile_sums.p);
+    scan_sums_kernel<<<1, kScanThreads, 0, s->stream>>>((int64_t *)s->tile_sums.p, ntiles, row_off + nleaf);
+    scan_add_kernel<<<grid_for(nleaf, 256, 1 << 30), 256, 0, s->stream>>>(row_off, nleaf, (int64_t *)s->tile_sums.p);
+    CUDA_TRY(cudaGetLastError());
+    launch_count(4);
+    int64_t total = 0;
+    int st = 0;
+    CUDA_TRY(cudaMemcpyAsync(&total, row_off + nleaf, sizeof(total), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(&st, status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (st & ST_WALK_TREE) return fail(P2P_ERR_ARG, "walk: a child code outside the tree");
+    if (st & ST_WALK_STACK) return fail(P2P_ERR_CAPACITY, "walk: a sink's walk exceeded its stack");
+    if (ntask) *ntask = total;
+    if (total == 0) return P2P_OK;
+    // pass 2: the rows' source ids, pair counts; then the pair kernel
+    P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)total));
+    const bool skip = skips_outside(s);
+    walk_rows_kernel<true><<<grid, threads, 0, s->stream>>>(
+        w, nullptr, row_off, (int *)s->row_src.p, s->d_np, (const LeafMeta *)s->meta.p,
+        0.5 / s->params.split_radius, (float)(s->fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin)),
+        (unsigned long long *)s->pairs.p, skip ? (unsigned long long *)s->skipped.p : nullptr, status);
+    CUDA_TRY(cudaGetLastError());
+    launch_count(1);
+    return enqueue_pairs(s, true);
+}
+
+P2P_API int p2p_pass_rows(p2p_session *s, int64_t *row_off, int *row_src) {
+    P2P_TRY(check_session(s));
+    if (s->in_pass) return fail(P2P_ERR_STATE, "pass still open; call p2p_pass_end first");
+    if (!row_off) return fail(P2P_ERR_ARG, "null argument");
+    const size_t nl = (size_t)s->nleaf + 1;
+    CUDA_TRY(cudaMemcpy(row_off, s->row_off.p, sizeof(int64_t) * nl, cudaMemcpyDeviceToHost));
+    const int64_t total = row_off[s->nleaf];
+    if (total > 0 && row_src)
+        CUDA_TRY(cudaMemcpy(row_src, s->row_src.p, sizeof(int) * (size_t)total, cudaMemcpyDeviceToHost));
     return P2P_OK;
 }
 

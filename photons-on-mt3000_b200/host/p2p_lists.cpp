@@ -510,6 +510,31 @@ void p2p_tree_leaves(const p2p_tree *h, int *ipart, int *npart, int *active, dou
     }
 }
 
+// Node table in node-id order for the device walk: child codes (2 per
+// node), the smallest leaf id of each subtree, centre and width (AoS).
+void p2p_tree_nodes(const p2p_tree *h, int *son, int *first_leaf, double *center, double *width) {
+    const Tree &T = h->T;
+    const int nn = (int)T.nodes.size();
+    if (first_leaf) {
+        // children have larger pre-order ids than their parent: fill bottom-up
+        for (int k = nn - 1; k >= 0; --k) {
+            const int c = T.nodes[k].son[0];
+            first_leaf[k] = is_node(c) ? first_leaf[cidx(c)] : cidx(c);
+        }
+    }
+    for (int k = 0; k < nn; ++k) {
+        const Node &nd = T.nodes[k];
+        if (son) {
+            son[2 * k] = nd.son[0];
+            son[2 * k + 1] = nd.son[1];
+        }
+        for (int d = 0; d < 3; ++d) {
+            if (center) center[3 * k + d] = nd.center[d];
+            if (width) width[3 * k + d] = nd.width[d];
+        }
+    }
+}
+
 namespace {
 // has_sink[node] = the subtree holds a leaf with active >= 0
 char mark_sinks(const Tree &T, int c, std::vector<char> &has) {

@@ -47,6 +47,7 @@ def lists():
         lib.p2p_tree_nnode.argtypes = [_vp]
         lib.p2p_tree_nnode.restype = ctypes.c_int
         lib.p2p_tree_leaves.argtypes = [_vp, _i32p, _i32p, _i32p, _f64p, _f64p]
+        lib.p2p_tree_nodes.argtypes = [_vp, _i32p, _i32p, _f64p, _f64p]
         lib.p2p_tree_walk.restype = ctypes.c_int64
         lib.p2p_tree_walk.argtypes = [_vp, ctypes.c_double, ctypes.c_double]
         lib.p2p_tree_tasks.argtypes = [_vp, _i32p, _i32p]

@@ -83,6 +83,21 @@ _i = ctypes.c_int
 _i64 = ctypes.c_int64
 _d = ctypes.c_double
 
+class WalkTree(ctypes.Structure):
+    """p2p_walk_tree: the kd-tree in device memory (pointers as integers)."""
+    _fields_ = [
+        ("nnode", ctypes.c_int),
+        ("nleaf", ctypes.c_int),
+        ("son", ctypes.c_void_p),
+        ("node_first", ctypes.c_void_p),
+        ("node_center", ctypes.c_void_p),
+        ("node_width", ctypes.c_void_p),
+        ("leaf_center", ctypes.c_void_p),
+        ("leaf_width", ctypes.c_void_p),
+        ("leaf_active", ctypes.c_void_p),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "p2p_params_default": (None, [ctypes.POINTER(Params)]),
@@ -105,6 +120,8 @@ SIGNATURES = {
     "p2p_pass_accumulate": (_i, [_vp, _vp]),
     "p2p_pass_result": (_i, [_vp, _vp]),
     "p2p_pass_result_device": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "p2p_pass_submit_walk": (_i, [_vp, ctypes.POINTER(WalkTree), _d, _d, ctypes.POINTER(_i64)]),
+    "p2p_pass_rows": (_i, [_vp, _vp, _vp]),
     "p2p_session_synchronize": (_i, [_vp]),
     "p2p_pass_pair_count": (_i, [_vp, ctypes.POINTER(_i64)]),
     "p2p_pass_evaluated_pairs": (_i, [_vp, ctypes.POINTER(_i64)]),

@@ -105,6 +105,18 @@ class Tree:
     def nleaf(self):
         return self.leaf_npart.shape[0]
 
+    def nodes(self):
+        """Node table for the device walk: (son (nnode, 2) child codes,
+        first leaf id per subtree, centres (nnode, 3), widths (nnode, 3))."""
+        nn = self.lib.p2p_tree_nnode(self.h)
+        son = np.empty((nn, 2), np.int32)
+        first = np.empty(nn, np.int32)
+        center = np.empty((nn, 3), np.float64)
+        width = np.empty((nn, 3), np.float64)
+        self.lib.p2p_tree_nodes(self.h, _ptr(son, _i32p), _ptr(first, _i32p), _ptr(center, _f64p),
+                                _ptr(width, _f64p))
+        return son, first, center, width
+
     def walk(self, cutoff, open_angle, leaf_mask=None):
         """(task_t, task_s) of the P2P walk (src/fmm.c:656-792); with
         leaf_mask (nleaf bools) only the rows of the masked sink leaves, in
@@ -135,6 +147,11 @@ class Tree:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def num_threads():
+    """Host threads the tree build and walk use (OpenMP)."""
+    return _native.lists().p2p_lists_num_threads()
 
 
 def build_tree_lists(pos, tag, maxleaf, boxsize, cutoff, open_angle, sink_particles=None):

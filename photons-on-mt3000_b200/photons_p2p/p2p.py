@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 
-from . import _native
+from . import _native, abi
 from .abi import (FORM_PLAIN_FP64, P2P_OK, SOFT_CLAMP, Params)
 
 
@@ -96,6 +96,7 @@ class Session:
             masses, mp = _host(masses, np.float64)
         self._keep = [pos, ip, npt, masses]
         self.npart = pos.shape[-1]
+        self._nleaf = ip.shape[0]
         _check(self.lib, self.lib.p2p_pass_begin(self.h, self.npart, pp, mp, ip.shape[0], ipp, npp))
 
     def submit(self, task_t, task_s):
@@ -144,9 +145,41 @@ class Session:
         self.accumulate(acc)
         return acc, sec
 
+    # -- device list walk ----------------------------------------------------
+    def submit_walk(self, tree_dev, cutoff, open_angle):
+        """Walks the P2P lists on the GPU into the open pass and launches the
+        pair kernel on them; tree_dev from device_walk_tree. Returns the
+        number of list entries."""
+        n = ctypes.c_int64()
+        _check(self.lib, self.lib.p2p_pass_submit_walk(self.h, ctypes.byref(tree_dev.struct), cutoff,
+                                                       open_angle, ctypes.byref(n)))
+        return n.value
+
+    def rows(self):
+        """(row_off, row_src) of the last submitted chunk or walk (host copies)."""
+        nleaf = self._nleaf
+        off = np.empty(nleaf + 1, np.int64)
+        _check(self.lib, self.lib.p2p_pass_rows(self.h, off.ctypes.data_as(ctypes.c_void_p), None))
+        src = np.empty(int(off[-1]), np.int32)
+        _check(self.lib, self.lib.p2p_pass_rows(self.h, off.ctypes.data_as(ctypes.c_void_p),
+                                                src.ctypes.data_as(ctypes.c_void_p)))
+        return off, src
+
+    def force_pass_walk(self, tree, tree_dev, cutoff, open_angle, masses=None):
+        """One pass on a lists.Tree's particles and leaves with the lists
+        walked on the GPU; returns (acc (3, npart) in tree order, gpu_seconds,
+        list entries)."""
+        self.begin(tree.pos, tree.leaf_ipart, tree.leaf_npart, masses)
+        ntask = self.submit_walk(tree_dev, cutoff, open_angle)
+        sec = self.end()
+        acc = np.zeros((3, self.npart), dtype=np.float64)
+        self.accumulate(acc)
+        return acc, sec, ntask
+
     # -- device-resident pass (pointers into HBM, e.g. torch tensors) --------
     def run_device(self, npart, d_pos, nleaf, d_ip, d_np, ntask, d_t, d_s, d_mass=None):
         self.npart = npart
+        self._nleaf = nleaf
         _check(self.lib, self.lib.p2p_pass_run_device(self.h, npart, d_pos, d_mass, nleaf, d_ip, d_np,
                                                       ntask, d_t, d_s))
 
@@ -168,3 +201,20 @@ class Session:
 
 def kernel_launch_count():
     return _native.core().p2p_kernel_launch_count()
+
+
+class DeviceWalkTree:
+    """A lists.Tree's node and leaf tables in device memory (torch tensors)
+    as the p2p_walk_tree the device walk reads."""
+
+    def __init__(self, tree, device):
+        import torch
+
+        son, first, center, width = tree.nodes()
+        to = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+        self._t = [to(son), to(first), to(center), to(width), to(tree.leaf_center), to(tree.leaf_width),
+                   to(tree.leaf_active)]
+        t = self._t
+        self.struct = abi.WalkTree(son.shape[0], tree.nleaf, t[0].data_ptr(), t[1].data_ptr(),
+                                   t[2].data_ptr(), t[3].data_ptr(), t[4].data_ptr(), t[5].data_ptr(),
+                                   t[6].data_ptr())

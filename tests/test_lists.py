@@ -113,3 +113,78 @@ def test_masked_walk_equals_filtered_walk(nsink):
     assert sel.any()
     assert np.array_equal(part.task_t, full.task_t[sel])
     assert np.array_equal(part.task_s, full.task_s[sel])
+
+
+def _acceptance(wi, wj, ci, cj, cutoff, open_angle):
+    """acceptance (src/fmm.c:409-479, LONGSHORT) in Python doubles."""
+    dist = [ci[d] - cj[d] for d in range(3)]
+    w = [(wi[d] + wj[d]) * 0.5 for d in range(3)]
+    dd2 = dist[0] * dist[0] + dist[1] * dist[1] + dist[2] * dist[2]
+    mn = [max(abs(dist[d]) - w[d], 0.0) for d in range(3)]
+    if mn[0] + mn[1] + mn[2] < 1e-15:
+        return 0
+    if mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2] > cutoff * cutoff:
+        return -1
+    wmax = abs(max(w)) * 2
+    return 1 if wmax * wmax < open_angle * open_angle * dd2 else 0
+
+
+def per_sink_rows(tree, cutoff, open_angle):
+    """The device walk's algorithm (csrc/p2p_walk_kernels.cuh) restated: for
+    each sink leaf, the part of the serial dual-tree walk whose sink side
+    holds it, depth first with children in the serial order."""
+    son, first, nc, nw = (a.tolist() for a in tree.nodes())
+    lc, lw, act = tree.leaf_center.tolist(), tree.leaf_width.tolist(), tree.leaf_active.tolist()
+    ctr = lambda c: nc[c >> 1] if c & 1 else lc[c >> 1]  # noqa: E731
+    wid = lambda c: nw[c >> 1] if c & 1 else lw[c >> 1]  # noqa: E731
+
+    def toward(a, leaf):
+        s0, s1 = son[a >> 1]
+        return s0 if leaf < (first[s1 >> 1] if s1 & 1 else s1 >> 1) else s1
+
+    rows = []
+    for leaf in range(tree.nleaf):
+        out, stack = [], ([(1, 1)] if act[leaf] >= 0 else [])
+        while stack:
+            a, b = stack.pop()
+            if a == b and not a & 1 or not (a & 1 or b & 1):
+                out.append(b >> 1)
+                continue
+            if a == b:
+                s0, s1 = son[a >> 1]
+                c = toward(a, leaf)
+                stack += [(c, s1), (c, s0)]
+                continue
+            if _acceptance(wid(a), wid(b), ctr(a), ctr(b), cutoff, open_angle) != 0:
+                continue
+            split_a = (a & 1) and (not b & 1 or sum(wid(a)) > sum(wid(b)))
+            if split_a:
+                stack.append((toward(a, leaf), b))
+            else:
+                s0, s1 = son[b >> 1]
+                stack += [(a, s1), (a, s0)]
+        rows.append(out)
+    return rows
+
+
+@pytest.mark.parametrize("config", ["c1", "ref_dropin"])
+def test_per_sink_walk_equals_sorted_serial_walk(config):
+    """Replaying the walk per sink leaf gives every sink's row of the serial
+    walk, entry for entry in the serial order (the rows a stable sort of the
+    serial list by sink builds): open angle 0 (cutoff-only lists) and the
+    reference's 0.4."""
+    cfg = W.c1_config() if config == "c1" else W.ref_dropin_config()
+    allpos, tag = W.with_ghosts(W.c1_positions(), cfg)
+    with L.Tree(allpos, tag, cfg.maxleaf, cfg.box) as tree:
+        tt, ts = tree.walk(cfg.cutoff_radius, cfg.open_angle)
+        rows = per_sink_rows(tree, cfg.cutoff_radius, cfg.open_angle)
+        son, first, _, _ = tree.nodes()
+    order = np.argsort(tt, kind="stable")
+    got_s = np.concatenate([np.asarray(r, np.int32) for r in rows])
+    got_t = np.repeat(np.arange(len(rows)), [len(r) for r in rows])
+    assert np.array_equal(got_t, tt[order]) and np.array_equal(got_s, ts[order])
+    # pre-order leaf numbering: son[0]'s leaves precede son[1]'s
+    s1 = son[:, 1]
+    f1 = s1 >> 1
+    f1[(s1 & 1) == 1] = first[f1[(s1 & 1) == 1]]
+    assert np.all(first < f1)
