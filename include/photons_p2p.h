@@ -167,7 +167,7 @@ typedef struct p2p_walk_tree {
 } p2p_walk_tree;
 /* Replaces the caller's walk_task_p2p (src/fmm.c:656-792, acceptance
  * src/fmm.c:409-479, called from fmm_task src/fmm.c:1221-1300) plus the
- * list submit: the P2P lists are walked on the GPU, one thread per sink leaf,
+ * list submit: the P2P lists are walked on the GPU, one warp per sink leaf,
  * straight into CSR rows equal entry for entry to those p2p_pass_submit
  * builds from the serial walk's list, then the pair kernel runs on them.
  * Within an open pass (its leaves are the tree's leaves). Waits for the row

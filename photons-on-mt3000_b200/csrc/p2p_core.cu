@@ -686,8 +686,8 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
     w.leaf_width = t->leaf_width;
     w.cutoff = cutoff;
     w.open_angle = open_angle;
-    const int threads = 128;
-    const int grid = grid_for(nleaf, threads, s->sm_count * 64);
+    const int threads = kWalkWarps * 32;
+    const int grid = grid_for(nleaf, kWalkWarps, s->sm_count * 32);
     int *status = (int *)s->status.p;
     // pass 1: row lengths, then the row offsets
     walk_rows_kernel<false><<<grid, threads, 0, s->stream>>>(w, (int *)s->counts.p, nullptr, nullptr, nullptr,
@@ -716,8 +716,15 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
         w, nullptr, row_off, (int *)s->row_src.p, s->d_np, (const LeafMeta *)s->meta.p,
         0.5 / s->params.split_radius, (float)(s->fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin)),
         (unsigned long long *)s->pairs.p, skip ? (unsigned long long *)s->skipped.p : nullptr, status);
+    // each row ascending by source leaf id: the serial walk's order for that sink
+    int *rs = (int *)s->row_src.p;
+    csr_sort_rows_warp_kernel<<<grid_for(nleaf, 4, s->sm_count * 8), 128, 0, s->stream>>>(row_off, nleaf, rs);
+    csr_sort_rows_block_kernel<<<grid_for(nleaf, 1, s->sm_count * 2), kSortBlockThreads, 0, s->stream>>>(
+        row_off, nleaf, rs);
+    csr_sort_rows_global_kernel<<<grid_for(nleaf, 1, s->sm_count), kSortBlockThreads, 0, s->stream>>>(
+        row_off, nleaf, rs);
     CUDA_TRY(cudaGetLastError());
-    launch_count(1);
+    launch_count(4);
     return enqueue_pairs(s, true);
 }
 

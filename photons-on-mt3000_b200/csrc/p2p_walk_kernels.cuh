@@ -4,13 +4,16 @@
 //
 // The serial walk recurses over leaf/node pairs (A, B) from (root, root). An
 // entry (L, S) is emitted when the recursion reaches two leaves. For a fixed
-// sink leaf L the pairs it visits on the way to its entries have A on L's
-// ancestor path, and which child of A the recursion takes is fixed by L; so
-// one thread per sink leaf replays exactly the part of the recursion whose
-// sink side contains L, depth first with the children in the serial order.
-// Its entries come out in the order the serial walk emits them for that sink,
-// which is the row order a stable sort of the serial list by sink gives: the
-// rows equal those the list path builds, entry for entry.
+// sink leaf L the pairs it visits on the way to L's entries have A on L's
+// ancestor path, and which child of A the recursion takes is fixed by L (the
+// child whose subtree holds L); how a pair expands depends on the pair alone.
+// So one warp per sink leaf expands that part of the recursion, its lanes
+// taking up to 32 pending pairs at a time from a shared-memory stack. The
+// serial walk emits a sink's sources in pre-order of the source side, i.e. in
+// increasing leaf id (leaves are numbered in pre-order and son[0]'s subtree is
+// walked before son[1]'s); sorting each row ascending afterwards therefore
+// gives the serial order, the row a stable sort of the serial list by sink
+// gives: the rows equal those the list path builds, entry for entry.
 //
 // The acceptance arithmetic is written with explicitly rounded FP64
 // operations (no contraction), the ISO C evaluation of the reference's code.
@@ -30,10 +33,8 @@ struct WalkArgs {
     double cutoff, open_angle;
 };
 
-constexpr int kWalkStack = 192;  // pending (A, B) pairs per sink leaf
-
 enum : int {
-    ST_WALK_STACK = 4,    // a sink's pending pairs exceeded kWalkStack (its row is cut short)
+    ST_WALK_STACK = 4,    // a sink's pending pairs exceeded the walk's stack (its row is cut short)
     ST_WALK_ROW = 8,      // the fill pass found more entries than the count pass
     ST_WALK_TREE = 16,    // a child code outside the tree, or a walk longer than any tree allows
 };
@@ -89,28 +90,34 @@ __device__ __forceinline__ int walk_child_toward(const WalkArgs &w, int A, int L
     return L < f1 ? w.son[2 * k] : s1;
 }
 
-// One thread per sink leaf. FILL = false: row lengths into counts[L].
-// FILL = true: the row's source ids into row_src[row_off[L] ...], the row's
-// pair count (and, with skipped, the pairs of entries wholly beyond the
-// FP32 forms' cutoff) added into *pairs / *skipped.
+constexpr int kWalkWarps = 4;         // warps (sink leaves in flight) per block
+constexpr int kWalkWarpStack = 1024;  // pending pairs per warp (shared memory)
+
+// One warp per sink leaf. FILL = false: row lengths into counts[L]. FILL =
+// true: the row's source ids into row_src[row_off[L] ...] (in the order the
+// warp finds them; the rows are sorted afterwards), the row's pair count (and,
+// with skipped, the pairs of entries wholly beyond the FP32 forms' cutoff)
+// added into *pairs / *skipped.
 template <bool FILL>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kWalkWarps * 32)
 walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__restrict__ row_off,
                  int *__restrict__ row_src, const int *__restrict__ leaf_npart,
                  const LeafMeta *__restrict__ meta, double cscale, float uout,
                  unsigned long long *__restrict__ pairs, unsigned long long *__restrict__ skipped,
                  int *__restrict__ status) {
+    __shared__ int2 stacks[kWalkWarps][kWalkWarpStack];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int2 *stk = stacks[wid];
     unsigned long long my_pairs = 0, my_skip = 0;
-    const int stride = gridDim.x * blockDim.x;
-    for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < w.nleaf; L += stride) {
-        if (w.leaf_active[L] < 0 || w.nnode <= 0) {
-            if (!FILL) counts[L] = 0;
+    for (int L = blockIdx.x * kWalkWarps + wid; L < w.nleaf; L += gridDim.x * kWalkWarps) {
+        if (w.leaf_active[L] < 0 || w.nnode <= 0) {  // warp-uniform
+            if (!FILL && lane == 0) counts[L] = 0;
             continue;
         }
-        int2 stack[kWalkStack];
-        int sp = 0;
-        stack[sp++] = make_int2(1, 1);  // (root, root): node 0
-        int n = 0;
+        if (lane == 0) stk[0] = make_int2(1, 1);  // (root, root): node 0
+        __syncwarp();
+        int sp = 1, n = 0, bad = 0;
         int64_t base = 0, cap = 0;
         LeafMeta mt{};
         long long np_t = 0;
@@ -120,82 +127,101 @@ walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__re
             np_t = leaf_npart[L];
             if (skipped) mt = meta[L];
         }
-        int bad = 0;
-        // a pair (A, B) is visited at most once per sink, A on the sink's
-        // ancestor path: any longer walk means a malformed tree
+        // every pair is visited at most once per sink: a longer walk means a
+        // malformed tree
         long long budget = 64LL * ((long long)w.nnode + w.nleaf) + 16;
-        auto emit = [&](int B) {
-            const int S = B >> 1;
-            if (FILL) {
-                if (n >= cap) {
-                    bad = ST_WALK_ROW;
-                    return;
-                }
-                row_src[base + n] = S;
-                const unsigned long long np = (unsigned long long)(np_t * (long long)leaf_npart[S]);
-                my_pairs += np;
-                if (skipped) {
-                    const LeafMeta ms = meta[S];
-                    float ox, oy, oz;
-                    entry_offset(ms, mt, cscale, ox, oy, oz);
-                    if (entry_u_min(ms, mt, ox, oy, oz) > uout) my_skip += np;
-                }
-            }
-            ++n;
-        };
-        auto push = [&](int A, int B) {
-            if (!walk_valid(w, A) || !walk_valid(w, B)) bad = ST_WALK_TREE;
-            else if (sp < kWalkStack) stack[sp++] = make_int2(A, B);
-            else bad = ST_WALK_STACK;
-        };
-        while (sp > 0 && !bad) {
-            if (--budget < 0) {
-                bad = ST_WALK_TREE;
-                break;
-            }
-            const int2 p = stack[--sp];
+        while (sp > 0) {
+            const int take = min(32, sp);
+            sp -= take;
+            budget -= take;
+            int2 p = make_int2(0, 0);
+            if (lane < take) p = stk[sp + lane];
+            __syncwarp();  // the batch is read before children overwrite it
             const int A = p.x, B = p.y;
-            if (A == B) {
-                if (!(A & 1)) {
-                    emit(B);
-                } else {
+            int nchild = 0, c0 = 0, c1 = 0, fault = 0;
+            bool emit = false;
+            if (lane < take) {
+                const bool a_node = A & 1, b_node = B & 1;
+                if ((A == B && !a_node) || (!a_node && !b_node)) {
+                    emit = true;
+                } else if (A == B) {
                     const int c = walk_child_toward(w, A, L);
                     const int k = A >> 1;
-                    push(c, w.son[2 * k + 1]);
-                    push(c, w.son[2 * k]);
-                }
-                continue;
-            }
-            const bool a_node = A & 1, b_node = B & 1;
-            if (!a_node && !b_node) {
-                emit(B);
-                continue;
-            }
-            // (the reference passes the leaf's width first in the node-leaf
-            // case; the sum of the two widths is the same either way)
-            const double *wa = walk_width(w, A), *wb = walk_width(w, B);
-            if (walk_acceptance(wa, wb, walk_center(w, A), walk_center(w, B), w.cutoff, w.open_angle) != 0)
-                continue;
-            if (!a_node) {  // leaf - node: both children of B, son[0] first
-                const int k = B >> 1;
-                push(A, w.son[2 * k + 1]);
-                push(A, w.son[2 * k]);
-            } else if (!b_node) {  // node - leaf: the child of A toward L
-                push(walk_child_toward(w, A, L), B);
-            } else {
-                const double sa = __dadd_rn(__dadd_rn(wa[0], wa[1]), wa[2]);
-                const double sb = __dadd_rn(__dadd_rn(wb[0], wb[1]), wb[2]);
-                if (sa > sb) {
-                    push(walk_child_toward(w, A, L), B);
+                    c0 = c;  // the pairs (c, son[0]) and (c, son[1]): second codes below
+                    nchild = 2;
+                    p = make_int2(w.son[2 * k], w.son[2 * k + 1]);
                 } else {
-                    const int k = B >> 1;
-                    push(A, w.son[2 * k + 1]);
-                    push(A, w.son[2 * k]);
+                    const double *wa = walk_width(w, A), *wb = walk_width(w, B);
+                    if (walk_acceptance(wa, wb, walk_center(w, A), walk_center(w, B), w.cutoff,
+                                        w.open_angle) == 0) {
+                        bool split_a = a_node && !b_node;
+                        if (a_node && b_node)
+                            split_a = __dadd_rn(__dadd_rn(wa[0], wa[1]), wa[2]) >
+                                      __dadd_rn(__dadd_rn(wb[0], wb[1]), wb[2]);
+                        if (split_a) {
+                            c0 = walk_child_toward(w, A, L);
+                            c1 = B;
+                            nchild = 1;
+                        } else {
+                            const int k = B >> 1;
+                            c0 = A;
+                            nchild = 2;
+                            p = make_int2(w.son[2 * k], w.son[2 * k + 1]);
+                        }
+                    }
                 }
             }
+            // children as (first, second) codes: nchild 1 -> (c0, c1);
+            // nchild 2 -> (c0, p.x), (c0, p.y)
+            int2 ch0 = nchild == 1 ? make_int2(c0, c1) : make_int2(c0, p.x);
+            int2 ch1 = make_int2(c0, p.y);
+            if (nchild >= 1 && (!walk_valid(w, ch0.x) || !walk_valid(w, ch0.y))) fault = ST_WALK_TREE;
+            if (nchild == 2 && !walk_valid(w, ch1.y)) fault = ST_WALK_TREE;
+            if (fault) nchild = 0;
+            int incl = nchild;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int v = __shfl_up_sync(kFull, incl, off);
+                if (lane >= off) incl += v;
+            }
+            const int total = __shfl_sync(kFull, incl, 31);
+            bad |= __reduce_or_sync(kFull, fault);
+            if (sp + total > kWalkWarpStack) {
+                bad |= ST_WALK_STACK;
+            } else {
+                const int at = sp + incl - nchild;
+                if (nchild >= 1) stk[at] = ch0;
+                if (nchild == 2) stk[at + 1] = ch1;
+                sp += total;
+            }
+            const unsigned em = __ballot_sync(kFull, emit);
+            if (emit) {
+                const int slot = n + __popc(em & lt);
+                const int S = B >> 1;
+                if (FILL) {
+                    if (slot < cap) {
+                        row_src[base + slot] = S;
+                        const unsigned long long np = (unsigned long long)(np_t * (long long)leaf_npart[S]);
+                        my_pairs += np;
+                        if (skipped) {
+                            const LeafMeta ms = meta[S];
+                            float ox, oy, oz;
+                            entry_offset(ms, mt, cscale, ox, oy, oz);
+                            if (entry_u_min(ms, mt, ox, oy, oz) > uout) my_skip += np;
+                        }
+                    }
+                }
+            }
+            n += __popc(em);
+            if (FILL && n > cap) bad |= ST_WALK_ROW;
+            if (budget < 0) bad |= ST_WALK_TREE;
+            __syncwarp();
+            if (bad) break;  // warp-uniform
         }
-        if (bad) atomicOr(status, bad);
-        if (!FILL) counts[L] = n;
+        if (lane == 0) {
+            if (!FILL) counts[L] = n;
+            if (bad) atomicOr(status, bad);
+        }
     }
     if (FILL) {
 #pragma unroll
@@ -203,7 +229,7 @@ walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__re
             my_pairs += __shfl_xor_sync(kFull, my_pairs, off);
             my_skip += __shfl_xor_sync(kFull, my_skip, off);
         }
-        if ((threadIdx.x & 31) == 0) {
+        if (lane == 0) {
             if (my_pairs) atomicAdd(pairs, my_pairs);
             if (skipped && my_skip) atomicAdd(skipped, my_skip);
         }

@@ -129,10 +129,11 @@ def _acceptance(wi, wj, ci, cj, cutoff, open_angle):
     return 1 if wmax * wmax < open_angle * open_angle * dd2 else 0
 
 
-def per_sink_rows(tree, cutoff, open_angle):
+def per_sink_rows(tree, cutoff, open_angle, batch=32):
     """The device walk's algorithm (csrc/p2p_walk_kernels.cuh) restated: for
     each sink leaf, the part of the serial dual-tree walk whose sink side
-    holds it, depth first with children in the serial order."""
+    holds it, expanded `batch` pending pairs at a time from a stack (one warp's
+    lanes), the row sorted ascending at the end."""
     son, first, nc, nw = (a.tolist() for a in tree.nodes())
     lc, lw, act = tree.leaf_center.tolist(), tree.leaf_width.tolist(), tree.leaf_active.tolist()
     ctr = lambda c: nc[c >> 1] if c & 1 else lc[c >> 1]  # noqa: E731
@@ -146,33 +147,29 @@ def per_sink_rows(tree, cutoff, open_angle):
     for leaf in range(tree.nleaf):
         out, stack = [], ([(1, 1)] if act[leaf] >= 0 else [])
         while stack:
-            a, b = stack.pop()
-            if a == b and not a & 1 or not (a & 1 or b & 1):
-                out.append(b >> 1)
-                continue
-            if a == b:
-                s0, s1 = son[a >> 1]
-                c = toward(a, leaf)
-                stack += [(c, s1), (c, s0)]
-                continue
-            if _acceptance(wid(a), wid(b), ctr(a), ctr(b), cutoff, open_angle) != 0:
-                continue
-            split_a = (a & 1) and (not b & 1 or sum(wid(a)) > sum(wid(b)))
-            if split_a:
-                stack.append((toward(a, leaf), b))
-            else:
-                s0, s1 = son[b >> 1]
-                stack += [(a, s1), (a, s0)]
-        rows.append(out)
+            take = min(batch, len(stack))
+            pending, stack = stack[len(stack) - take:], stack[:len(stack) - take]
+            for a, b in pending:
+                if a == b and not a & 1 or not (a & 1 or b & 1):
+                    out.append(b >> 1)
+                elif a == b:
+                    c = toward(a, leaf)
+                    stack += [(c, son[a >> 1][0]), (c, son[a >> 1][1])]
+                elif _acceptance(wid(a), wid(b), ctr(a), ctr(b), cutoff, open_angle) == 0:
+                    if (a & 1) and (not b & 1 or sum(wid(a)) > sum(wid(b))):
+                        stack.append((toward(a, leaf), b))
+                    else:
+                        stack += [(a, son[b >> 1][0]), (a, son[b >> 1][1])]
+        rows.append(sorted(out))
     return rows
 
 
 @pytest.mark.parametrize("config", ["c1", "ref_dropin"])
 def test_per_sink_walk_equals_sorted_serial_walk(config):
-    """Replaying the walk per sink leaf gives every sink's row of the serial
+    """Expanding the walk per sink leaf gives every sink's row of the serial
     walk, entry for entry in the serial order (the rows a stable sort of the
-    serial list by sink builds): open angle 0 (cutoff-only lists) and the
-    reference's 0.4."""
+    serial list by sink builds; the serial order of a row is increasing source
+    leaf id): open angle 0 (cutoff-only lists) and the reference's 0.4."""
     cfg = W.c1_config() if config == "c1" else W.ref_dropin_config()
     allpos, tag = W.with_ghosts(W.c1_positions(), cfg)
     with L.Tree(allpos, tag, cfg.maxleaf, cfg.box) as tree:
