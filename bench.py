@@ -280,10 +280,18 @@ def run_ours(args, rank, world, dist):
             raise RuntimeError(sess.lib.p2p_last_error().decode())
         return out
 
+    # launch shape: the autotuner's pick for this leaf-size histogram (FP32 forms)
+    prm, tuned = params_for(cfg, form, mass), None
+    if form != abi.FORM_PLAIN_FP64 and not args.no_tune:
+        from photons_p2p import autotune
+
+        prm, rec = autotune.tune(cfg, tl, form, mass, device=local, sample_pairs=args.tune_pairs,
+                                 cache_path=args.tune_cache)
+        tuned = {k: rec[k] for k in ("key", "variant", "stage", "warps", "sample_pairs", "cached")}
     with Session(local) as sess:
         fp32_peak = sess.measure_fp32_peak()
         fp64_peak = sess.measure_fp64_peak()
-        sess.set_params(params_for(cfg, form, mass))
+        sess.set_params(prm)
         degree = sess.poly_degree
         sampler = ClockSampler(local)
         pass_s, kern_ms, launches = resident_passes(sess, args.steps, args.warmup, sampler)
@@ -305,7 +313,7 @@ def run_ours(args, rank, world, dist):
             rel = num / np.where(den > 0, den, 1.0)
             accuracy = {"vs": "plain_fp64", "rms": float(np.sqrt(np.mean(rel ** 2))),
                         "max": float(rel.max()), "particles": int(loc.sum())}
-            sess.set_params(params_for(cfg, form, mass))
+            sess.set_params(prm)
 
         # e2e through the C ABI on pinned host buffers
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -367,7 +375,8 @@ def run_ours(args, rank, world, dist):
                    "leaf_cap": cfg.maxleaf, "mesh": cfg.mesh,
                    "r_s": cfg.split_radius, "x_cut": cfg.x_cut, "eps": cfg.eps, "soft": "plummer"
                    if cfg.soft_mode == abi.SOFT_PLUMMER else "clamp", "open_angle": cfg.open_angle,
-                   "poly_degree": degree, "parallelism": f"replicas x{world}",
+                   "poly_degree": degree, "launch_shape": tuned or "default",
+                   "parallelism": f"replicas x{world}",
                    "l2": "256 MB flush between steps; inputs > L2", "host_prep_s": round(prep_s, 1)},
         "kernel_ms": mean_kernel_ms,
         "kernel_pairs_per_s": kernel_pairs_per_s,
@@ -659,6 +668,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary")
     ap.add_argument("--no-walk", action="store_true", help="skip the device list walk leg")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shape, no autotuning")
     ap.add_argument("--boxes", type=int, default=512, help="c4: ensemble size")
     ap.add_argument("--slots", type=int, default=1, help="c4: server launch slots")
     ap.add_argument("--hbm-gb", type=float, default=100.0, help="c4: server arena size")
