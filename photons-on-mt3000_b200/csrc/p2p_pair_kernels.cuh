@@ -237,7 +237,7 @@ pair_split_kernel(const __grid_constant__ PairArgs a, const int stage_cap) {
 // (or Kahan / FP32) total.
 constexpr int kSinkGroup = 4;        // sinks evaluated per predicated block
 #ifndef P2P_FLUSH_CHUNKS
-#define P2P_FLUSH_CHUNKS 32
+#define P2P_FLUSH_CHUNKS 64
 #endif
 constexpr int kSrcFlushChunks = P2P_FLUSH_CHUNKS;  // FP32 partial depth per lane, in chunks
 
