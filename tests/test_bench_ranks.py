@@ -56,3 +56,20 @@ def test_combine_single_process():
     import bench
 
     assert bench.combine_ranks(2.0, 3.0, 7, None, "cpu") == (2.0, 3.0, 7.0)
+
+
+def test_plain_roofline_uses_committed_fp64_count():
+    """The plain form's roofline: FP64 flops per pair from the committed ncu
+    count, against the FP64 peak and the FP32 peak; no count, no figure."""
+    import sys
+
+    sys.path.insert(0, REPO)
+    import bench
+
+    f64 = bench.load_fp64_flops("c2")
+    assert f64 and 100 < f64 < 400
+    r = bench.plain_roofline("c2", 2.0e11, 2000.0, 34.0, 72.0)
+    achieved = 2.0e11 / 2.0 * f64 / 1e12
+    assert abs(r["achieved"] - achieved) < 1e-9 * achieved
+    assert abs(r["frac"] - achieved / 34.0) < 1e-12 and abs(r["frac_of_fp32_peak"] - achieved / 72.0) < 1e-12
+    assert bench.plain_roofline("no_such_workload", 1.0, 1.0, 34.0, 72.0)["flops_per_pair"] is None
