@@ -91,6 +91,8 @@ void begin_pass() {
     const int n = NPART;
     const int nleaf = last_leaf - first_leaf;
     std::vector<double> pos(3 * (size_t)n);
+    // (the reference packs on one thread; the iterations are independent)
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         for (int d = 0; d < 3; ++d) {
 #ifndef INTXYZ
@@ -132,6 +134,7 @@ void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time)
     }
     if (ntask > 0) {
         // devMemcpyHD_task rebases the caller's arrays in place (src/gpu_func.impl.h:704-713)
+#pragma omp parallel for schedule(static)
         for (int j = 0; j < ntask; ++j) {
             ltask_t[j] -= first_leaf;
             ltask_s[j] -= first_leaf;
@@ -211,6 +214,7 @@ void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
     const int n = NPART;
     for (int p = 0; p < npack; ++p) {
         if (packs[p].ntask == 0) continue;
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < packs[p].npart; ++i) {
             const int j = packs[p].ipart + i;
             if (active_level == -1 || (active_level && part[j].act == active_level)) {
