@@ -47,6 +47,8 @@ def test_null_arguments_are_rejected():
     assert lib.p2p_session_create(0, None) == abi.P2P_ERR_ARG
     assert lib.p2p_session_set_params(None, None) == abi.P2P_ERR_ARG
     assert lib.p2p_pass_end(None, None) == abi.P2P_ERR_ARG
+    assert lib.p2p_pass_submit_walk(None, None, 1.0, 0.0, None) == abi.P2P_ERR_ARG
+    assert lib.p2p_pass_rows(None, None, None) == abi.P2P_ERR_ARG
     assert b"null" in lib.p2p_last_error()
 
 
