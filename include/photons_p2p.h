@@ -83,6 +83,10 @@ typedef struct {
                                              more resident warps; for small leaves) */
 #define P2P_VARIANT_SINK_LANES_X2 5       /* packed sink lanes: each lane keeps a sink pair,
                                              the leaf's pairs share the lanes' sources */
+#define P2P_VARIANT_SINK_REGS 6           /* each lane keeps four sinks in registers (two packed
+                                             pairs) and takes every J-th staged source; sources
+                                             are classified per particle against the sink slice's
+                                             box (dropped / no cutoff test / cutoff test) */
 
 typedef struct p2p_session p2p_session;
 
@@ -139,7 +143,10 @@ int p2p_pass_pair_count(p2p_session *s, int64_t *pairs);
 /* No counterpart in the reference: of those, the pair interactions the
  * kernels evaluated. The packed FP32 kernels skip list entries whose
  * particles' bounding boxes lie wholly beyond the cutoff (all their pairs
- * would be dropped, so the result is the same); the count excludes them. */
+ * would be dropped, so the result is the same); the count excludes them.
+ * The sink-register kernel also drops single source particles that lie
+ * beyond the cutoff from every sink of a slice, and counts on the device the
+ * pairs it evaluates (staged sources times the slice's sinks). */
 int p2p_pass_evaluated_pairs(p2p_session *s, int64_t *pairs);
 
 /* Whole pass on device-resident inputs in one call, enqueued on the session

@@ -24,7 +24,10 @@ inline void fill_pass_scalars(PairArgs &a, const p2p_params &p, const PolyFit &f
     a.ucut_hi = (float)(fit.umax * (1.0 + kCutBand));
     a.rcut2 = fit.umax / (c * c);
     a.eps2_box = p.soften * p.soften;
-    for (int k = 0; k < kMaxCoef; ++k) a.coef[k] = -fit.coef[k];
+    for (int k = 0; k < kMaxCoef; ++k) {
+        a.coef[k] = -fit.coef[k];
+        a.coef2[k] = make_float2(a.coef[k], a.coef[k]);
+    }
     a.uin = (float)(fit.umax * (1.0 - kInsideMargin));
     a.uout = (float)(fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin));
     a.out_scale = c * c * (per_particle_masses ? 1.0 : p.mass);

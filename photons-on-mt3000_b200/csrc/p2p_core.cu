@@ -87,7 +87,7 @@ struct p2p_session {
     // device buffers
     DevBuf task_t2, task_s2;  // second buffer pair of pipelined submits
     DevBuf pos, mass, leaf_ip, leaf_np, task_t, task_s, meta, pos4, counts, fill, row_off,
-        row_src, tile_sums, acc, status, queue, pairs, skipped, probe;
+        row_src, tile_sums, acc, status, queue, pairs, skipped, evaluated, probe;
     DevBuf keys_a, keys_b, vals_b, hist, hoffs, hsums;  // radix sort of the list
     // pass state
     bool in_pass = false;
@@ -155,7 +155,7 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 1024]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
-    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SINK_LANES_X2)
+    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SINK_REGS)
         return fail(P2P_ERR_ARG, "unknown kernel_variant %d", p->kernel_variant);
     if (p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES &&
         p->warps_per_block > 4)
@@ -164,8 +164,9 @@ int validate_params(const p2p_params *p) {
         const int w = p->warps_per_block ? p->warps_per_block : 4;
         const int st = p->stage_sources ? p->stage_sources : (p->form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
         const size_t smem = p->form == P2P_FORM_PLAIN_FP64 ? pair_smem_plain(w, st)
-                            : std::max(std::max(pair_smem_x2(w, st), pair_smem_sx2(w, st)),
-                                       pair_smem_split(w, st, true));
+                            : std::max(std::max(std::max(pair_smem_x2(w, st), pair_smem_sx2(w, st)),
+                                                pair_smem_split(w, st, true)),
+                                       pair_smem_sreg(w, st));
         if (smem > (size_t)227 * 1024)
             return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
     }
@@ -185,6 +186,12 @@ bool packed_lanes(const p2p_params &p) {
     return p.form != P2P_FORM_PLAIN_FP64 &&
            (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2 ||
             p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16);
+}
+
+// Whether the pair kernel counts the pairs it evaluates on the device (the
+// sink-register kernel, which also drops single source particles).
+bool counts_evaluated(const p2p_params &p) {
+    return is_fp32_form(p.form) && p.kernel_variant == P2P_VARIANT_SINK_REGS;
 }
 
 int default_stage(const p2p_params &p) {
@@ -212,6 +219,8 @@ int launch_pair(p2p_session *s, const PairArgs &a) {
         r = launch_pair_plain(L, a);
     else if (p.kernel_variant == P2P_VARIANT_SINK_LANES_X2)
         r = launch_pair_sink_lanes_x2(L, a);
+    else if (p.kernel_variant == P2P_VARIANT_SINK_REGS)
+        r = launch_pair_sink_regs(L, a);
     else if (packed_lanes(p))
         r = launch_pair_source_lanes_x2(L, a);
     else if (source_lanes(p))
@@ -231,6 +240,7 @@ cudaError_t allow_smem_all() {
     if (e == cudaSuccess) e = allow_smem_source_lanes();
     if (e == cudaSuccess) e = allow_smem_source_lanes_x2();
     if (e == cudaSuccess) e = allow_smem_sink_lanes_x2();
+    if (e == cudaSuccess) e = allow_smem_sink_regs();
     if (e == cudaSuccess) e = allow_smem_plain();
     return e;
 }
@@ -280,6 +290,7 @@ PairArgs make_args(p2p_session *s) {
     a.mass = s->d_mass;
     a.acc = (double *)s->acc.p;
     a.queue = (int *)s->queue.p;
+    a.evaluated = counts_evaluated(p) ? (unsigned long long *)s->evaluated.p : nullptr;
     a.npart = s->npart;
     a.nleaf = s->nleaf;
     fill_pass_scalars(a, p, s->fit, s->d_mass != nullptr);
@@ -306,6 +317,7 @@ bool skips_outside(const p2p_session *s) {
     return packed_lanes(s->params) ||
            (is_fp32_form(s->params.form) && s->params.kernel_variant == P2P_VARIANT_SINK_LANES_X2);
 }
+
 
 // CSR build + pair kernel for one list chunk already on the device.
 int enqueue_chunk(p2p_session *s, int64_t ntask, const int *d_t, const int *d_s, bool timed,
@@ -373,6 +385,7 @@ int size_pass_buffers(p2p_session *s, int npart, int nleaf, bool host_inputs, bo
     P2P_TRY(ensure(s, s->queue, sizeof(int)));
     P2P_TRY(ensure(s, s->pairs, sizeof(unsigned long long)));
     P2P_TRY(ensure(s, s->skipped, sizeof(unsigned long long)));
+    P2P_TRY(ensure(s, s->evaluated, sizeof(unsigned long long)));
     return P2P_OK;
 }
 
@@ -381,6 +394,7 @@ int begin_common(p2p_session *s) {
     CUDA_TRY(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
     CUDA_TRY(cudaMemsetAsync(s->pairs.p, 0, sizeof(unsigned long long), s->stream));
     CUDA_TRY(cudaMemsetAsync(s->skipped.p, 0, sizeof(unsigned long long), s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->evaluated.p, 0, sizeof(unsigned long long), s->stream));
     return enqueue_prep(s);
 }
 
@@ -484,7 +498,7 @@ P2P_API int p2p_session_destroy(p2p_session *s) {
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     DevBuf *bufs[] = {&s->pos, &s->mass, &s->leaf_ip, &s->leaf_np, &s->task_t, &s->task_s,
                       &s->meta, &s->pos4, &s->counts, &s->fill, &s->row_off, &s->row_src,
-                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->skipped, &s->probe,
+                      &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->skipped, &s->evaluated, &s->probe,
                       &s->keys_a, &s->keys_b, &s->vals_b, &s->hist, &s->hoffs, &s->hsums,
                       &s->task_t2, &s->task_s2};
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
@@ -777,6 +791,11 @@ P2P_API int p2p_pass_evaluated_pairs(p2p_session *s, int64_t *pairs) {
     if (!pairs) return fail(P2P_ERR_ARG, "null argument");
     unsigned long long v = 0, k = 0;
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (counts_evaluated(s->params)) {
+        CUDA_TRY(cudaMemcpy(&v, s->evaluated.p, sizeof(v), cudaMemcpyDeviceToHost));
+        *pairs = (int64_t)v;
+        return P2P_OK;
+    }
     CUDA_TRY(cudaMemcpy(&v, s->pairs.p, sizeof(v), cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(&k, s->skipped.p, sizeof(k), cudaMemcpyDeviceToHost));
     *pairs = (int64_t)(v - k);

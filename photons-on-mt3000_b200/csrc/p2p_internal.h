@@ -3,6 +3,8 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 namespace p2p {
 
 // Per-leaf record the pair kernels read for every source entry: the FP64
@@ -51,6 +53,7 @@ struct PairArgs {
     const double *mass;      // FP64 form: per-particle masses or null
     double *acc;             // SoA 3 * npart, +=
     int *queue;              // persistent work counter (reset to 0 before launch)
+    unsigned long long *evaluated;  // nullable: += pair interactions the kernel evaluated
     int npart, nleaf;
     // FP32 forms (scaled units: lengths times c = 1 / (2 r_s))
     float eps2;              // (c * eps)^2
@@ -65,6 +68,8 @@ struct PairArgs {
     double cscale;           // c
     double out_scale;        // c^2 * mass (equal masses) or c^2 (per-particle masses)
     float coef[kMaxCoef];    // -H(u) ~ sum coef[k] (u - u0)^k (negated, so f = rinv^2 * rinv + poly)
+    float2 coef2[kMaxCoef];  // the same as (coef[k], coef[k]): packed FMA operands read from the
+                             // constant bank as they are, with no register pair to build
     float uin;               // entries whose bound on u stays below uin hold no cutoff-band pair
     float uout;              // entries whose lower bound on u exceeds uout hold no kept pair
     // FP64 form (reference units)

@@ -45,6 +45,13 @@ inline size_t pair_smem_plain(int warps, int stage) { return (size_t)warps * sta
 inline size_t pair_smem_x2(int warps, int stage) { return (size_t)warps * (stage + 64 + stage / 4) * 16; }
 // packed sink-lane kernel: staged sources as two float4 + index, 32 padding slots
 inline size_t pair_smem_sx2(int warps, int stage) { return (size_t)warps * (stage + 32) * 36; }
+// sink-register kernel: staged sources (pre-duplicated, with their indices) + lane
+// accumulators + staging context; its stage holds at least kSregMinStage sources (one staging group)
+constexpr int kSregMinStage = 128;
+inline int sreg_stage(int stage) { return stage < kSregMinStage ? kSregMinStage : stage; }
+inline size_t pair_smem_sreg(int warps, int stage) {
+    return (size_t)warps * ((size_t)sreg_stage(stage) * 32 + 12 * 32 * 8 + 1024);
+}
 
 // Persistent grid for `kernel`: blocks_per_sm, or as many as registers and
 // shared memory let reside (queried once and cached).
@@ -87,6 +94,7 @@ PairLaunchResult launch_pair_sink_lanes(const PairLaunch &L, const PairArgs &a);
 PairLaunchResult launch_pair_source_lanes(const PairLaunch &L, const PairArgs &a);
 PairLaunchResult launch_pair_source_lanes_x2(const PairLaunch &L, const PairArgs &a);
 PairLaunchResult launch_pair_sink_lanes_x2(const PairLaunch &L, const PairArgs &a);
+PairLaunchResult launch_pair_sink_regs(const PairLaunch &L, const PairArgs &a);
 // FP64 form.
 PairLaunchResult launch_pair_plain(const PairLaunch &L, const PairArgs &a);
 
@@ -95,6 +103,7 @@ cudaError_t allow_smem_sink_lanes();
 cudaError_t allow_smem_source_lanes();
 cudaError_t allow_smem_source_lanes_x2();
 cudaError_t allow_smem_sink_lanes_x2();
+cudaError_t allow_smem_sink_regs();
 cudaError_t allow_smem_plain();
 
 }  // namespace p2p

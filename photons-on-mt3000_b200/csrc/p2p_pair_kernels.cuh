@@ -414,24 +414,24 @@ constexpr int kTailGroup = P2P_X2_TAILGROUP;
 // coefficient pairs held in registers or read as f32x2 parameters.)
 template <int NC>
 __device__ __forceinline__ float2 poly_x2(const float2 t, const PairArgs &a) {
-    float2 h = make_float2(a.coef[NC - 1], a.coef[NC - 1]);
+    float2 h = a.coef2[NC - 1];
 #pragma unroll
-    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, make_float2(a.coef[k], a.coef[k]));
+    for (int k = NC - 2; k >= 0; --k) h = __ffma2_rn(h, t, a.coef2[k]);
     return h;
 }
 
 // CHECK = false: every pair is known to be inside the cutoff (no select).
 // CHECK = true: pairs beyond the band are dropped, pairs inside the band are
 // flagged in amb for an FP64 decision.
+// Sink pair given as packed negated coordinates (nx, ny, nz).
 template <int SOFT, bool MASSES, int NC, bool CHECK>
-__device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
-                                              const float sw, const SinkPair &p,
-                                              const PairArgs &a, const float2 eps2v,
-                                              const float2 negu0v, float2 &ax, float2 &ay,
-                                              float2 &az, bool &amb) {
-    const float2 dx = __fadd2_rn(sx, make_float2(p.xy.x, p.xy.y));
-    const float2 dy = __fadd2_rn(sy, make_float2(p.xy.z, p.xy.w));
-    const float2 dz = __fadd2_rn(sz, p.z);
+__device__ __forceinline__ void pair_split_x2n(const float2 sx, const float2 sy, const float2 sz, const float sw,
+                                               const float2 nx, const float2 ny, const float2 nz, const PairArgs &a,
+                                               const float2 eps2v, const float2 negu0v, float2 &ax, float2 &ay,
+                                               float2 &az, bool &amb) {
+    const float2 dx = __fadd2_rn(sx, nx);
+    const float2 dy = __fadd2_rn(sy, ny);
+    const float2 dz = __fadd2_rn(sz, nz);
     float2 u;
     if (SOFT == SOFT_PLUMMER) {
         u = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2v)));
@@ -454,6 +454,16 @@ __device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, 
     ax = __ffma2_rn(dx, f, ax);
     ay = __ffma2_rn(dy, f, ay);
     az = __ffma2_rn(dz, f, az);
+}
+
+template <int SOFT, bool MASSES, int NC, bool CHECK>
+__device__ __forceinline__ void pair_split_x2(const float2 sx, const float2 sy, const float2 sz,
+                                              const float sw, const SinkPair &p,
+                                              const PairArgs &a, const float2 eps2v,
+                                              const float2 negu0v, float2 &ax, float2 &ay,
+                                              float2 &az, bool &amb) {
+    pair_split_x2n<SOFT, MASSES, NC, CHECK>(sx, sy, sz, sw, make_float2(p.xy.x, p.xy.y), make_float2(p.xy.z, p.xy.w),
+                                            p.z, a, eps2v, negu0v, ax, ay, az, amb);
 }
 
 // One pair whose FP32 u fell in the cutoff band: decide inclusion from the

@@ -23,6 +23,7 @@ VARIANT_SOURCE_LANES = 2
 VARIANT_SOURCE_LANES_X2 = 3
 VARIANT_SOURCE_LANES_X2_S16 = 4
 VARIANT_SINK_LANES_X2 = 5
+VARIANT_SINK_REGS = 6
 
 FORM_NAMES = {
     FORM_PLAIN_FP64: "plain_fp64",

@@ -74,7 +74,7 @@ def test_plain_matches_oracle_c1_plummer(gpu, c1):
 
 
 VARIANTS = [abi.VARIANT_SINK_LANES, abi.VARIANT_SOURCE_LANES, abi.VARIANT_SOURCE_LANES_X2,
-            abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2]
+            abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2, abi.VARIANT_SINK_REGS]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -261,7 +261,8 @@ def test_run_device_graph_matches_host_path(gpu, dropin32):
             assert s.pair_count() == tl.pair_count()
 
 
-@pytest.mark.parametrize("variant", [abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SINK_LANES_X2])
+@pytest.mark.parametrize("variant", [abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SINK_LANES_X2,
+                                     abi.VARIANT_SINK_REGS])
 def test_skipped_entries_change_nothing(gpu, c1, variant):
     """The packed kernels skip list entries whose particles lie wholly beyond
     the cutoff. The skipped pairs are counted (evaluated <= listed, and some
