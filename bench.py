@@ -15,6 +15,8 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
            L2 flushed between steps (inputs are also larger than L2)
   accuracy the chosen form's per-particle force error against the plain
            FP64 form on the same inputs (rms and max of |da| / |a|)
+  accuracy_vs_oracle  the chosen and the plain form against the FP64 direct
+           minimum-image sum (the oracle) on 10^4 random local sinks
   e2e      the same metric through the C ABI on pinned host buffers:
            H2D of positions, leaves and lists, the pass, D2H of the forces
   roofline FP32 pipe: pairs/s x flops-per-pair (counted from the kernel
@@ -31,7 +33,10 @@ independent box (replicas, no collective on the data path); the timed
 region is bracketed by barriers and the max over ranks is reported.
 --impl reference times the reference's own P2P arithmetic (P2P_core_lite,
 FP32 SPI, compiled for the host from the reference sources into
-oracle/_ref) on the host cores, over a bounded sample of the same lists.
+oracle/_ref) on the host cores, over a bounded sample of the same lists:
+the rows of every k-th sink leaf, about 2e9 pair interactions (the default
+run's cpu_baseline is the same sample, with the first sink rows' figure
+beside it).
 """
 import argparse
 import ctypes
@@ -297,6 +302,7 @@ def run_ours(args, rank, world, dist):
         pass_s, kern_ms, launches = resident_passes(sess, args.steps, args.warmup, sampler)
         clocks = sampler.summary()
         acc_form = result(sess)
+        acc_plain = None
         evaluated = sess.evaluated_pairs()
         # the plain FP64 form on the same inputs: the split/plain ratio and the
         # chosen form's force error against it (local particles)
@@ -390,7 +396,10 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    return out, cfg, tl, nlocal
+    forms = {abi.FORM_NAMES[form]: acc_form}
+    if acc_plain is not None:
+        forms["plain_fp64"] = acc_plain
+    return out, cfg, tl, nlocal, raw_pos, forms
 
 
 C4_EPS_OVER_RS = (1.0 / 40) / 1.2  # serving boxes: eps = 1/(40 n), r_s = 1.2 / n
@@ -614,22 +623,30 @@ class _Null:
         return False
 
 
-def cpu_reference_sample(cfg, tl, mass, target_pairs):
-    """The list entries of the first sink leaves (leaf-id order) whose rows
-    add up to about target_pairs pair interactions."""
+def cpu_reference_sample(cfg, tl, mass, target_pairs, strided=True):
+    """A bounded sample of the pass for the CPU legs, about target_pairs pair
+    interactions of whole sink rows: strided, the rows of every k-th sink
+    leaf across the whole box (the autotuner's sample); else the rows of the
+    first sink leaves in leaf-id order (one corner of the box)."""
+    if strided:
+        from photons_p2p import autotune
+
+        tt, ts, pairs = autotune.sample_rows(tl.leaf_npart, tl.task_t, tl.task_s, target_pairs)
+        k = max(1, int(tl.pair_count() // max(target_pairs, 1.0)))
+        return tt, ts, pairs, f"rows of every {k}-th sink leaf"
     npart = tl.leaf_npart.astype(np.int64)
     per_sink = np.bincount(tl.task_t, weights=(npart[tl.task_t] * npart[tl.task_s]).astype(np.float64),
                            minlength=tl.nleaf)
     cum = np.cumsum(per_sink)
     last = min(int(np.searchsorted(cum, target_pairs)), tl.nleaf - 1)
     sel = tl.task_t <= last
-    return tl.task_t[sel], tl.task_s[sel], int(round(cum[last]))
+    return tl.task_t[sel], tl.task_s[sel], int(round(cum[last])), "first sink rows"
 
 
-def time_cpu(cfg, tl, mass, target_pairs, steps=1):
+def time_cpu(cfg, tl, mass, target_pairs, steps=1, strided=True):
     from oracle import oracle as O
 
-    tt, ts, pairs = cpu_reference_sample(cfg, tl, mass, target_pairs)
+    tt, ts, pairs, how = cpu_reference_sample(cfg, tl, mass, target_pairs, strided)
     if O.ref_available("libref_pair.so"):
         kind = "reference"
         soft = 0 if cfg.soft_mode == abi.SOFT_CLAMP else 1
@@ -652,7 +669,32 @@ def time_cpu(cfg, tl, mass, target_pairs, steps=1):
         times.append(time.perf_counter() - a)
     v = pairs / float(np.mean(times))
     return {"value": v, "unit": "pairs/s", "cores": O.num_threads(), "kind": kind,
-            "sample": f"{pairs:.3g} pair interactions ({len(tt)} list entries, first sink rows of {cfg.name}); {what}"}, times
+            "sample": f"{pairs:.3g} pair interactions ({len(tt)} list entries, {how} of {cfg.name}); {what}"}, times
+
+
+def accuracy_vs_oracle(cfg, raw_pos, tl, mass, forms, nsink=10000, seed=91):
+    """Per-particle relative force error of each form's pass against the FP64
+    direct minimum-image sum of the same truncated kernel (the oracle,
+    oracle/p2p_oracle.c oracle_direct), on nsink randomly drawn local sinks.
+    forms: {name: (3, npart) result in tree order}."""
+    from oracle import oracle as O
+
+    n = raw_pos.shape[1]
+    sinks = np.sort(np.random.default_rng(seed).choice(n, min(nsink, n), replace=False)).astype(np.int32)
+    prm = O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass)
+    t0 = time.time()
+    ref = O.direct(prm, raw_pos, cfg.box, sinks)
+    slot = np.empty(tl.npart, np.int64)
+    slot[tl.perm] = np.arange(tl.npart)
+    den = np.linalg.norm(ref, axis=0)
+    out = {"vs": "fp64 direct minimum-image sum (oracle)", "sinks": int(sinks.size),
+           "oracle_s": round(time.time() - t0, 1)}
+    for name, acc in forms.items():
+        if acc is None:
+            continue
+        rel = np.linalg.norm(acc[:, slot[sinks]] - ref, axis=0) / np.where(den > 0, den, 1.0)
+        out[name] = {"rms": float(np.sqrt(np.mean(rel ** 2))), "max": float(rel.max())}
+    return out
 
 
 def main():
@@ -733,12 +775,19 @@ def main():
             dist.destroy_process_group()
         return
 
-    out, cfg, tl, nlocal = run_ours(args, rank, world, dist)
+    out, cfg, tl, nlocal, raw_pos, forms = run_ours(args, rank, world, dist)
     if world == 1 and not args.no_serving and args.workload == "c2":
         out["serving"] = run_serving_leg(int(os.environ.get("LOCAL_RANK", "0")))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU leg: the reference's own pair arithmetic timed on the host
+        # cores over a strided sample (the first-rows sample beside it), and
+        # the oracle as the checker of the GPU forms' results
         cb, _ = time_cpu(cfg, tl, 1.0 / nlocal, args.cpu_pairs)
+        first, _ = time_cpu(cfg, tl, 1.0 / nlocal, args.cpu_pairs, strided=False)
+        cb["first_rows_value"] = first["value"]
+        cb["first_rows_sample"] = first["sample"]
         out["cpu_baseline"] = cb
+        out["accuracy_vs_oracle"] = accuracy_vs_oracle(cfg, raw_pos, tl, 1.0 / nlocal, forms)
     elif rank == 0:
         out["cpu_baseline"] = None
     if rank == 0:

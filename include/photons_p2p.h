@@ -125,7 +125,11 @@ int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *m
 /* Same with device pointers (already resident in HBM; not copied). */
 int p2p_pass_begin_device(p2p_session *s, int npart, const double *d_pos, const double *d_masses,
                           int nleaf, const int *d_leaf_ipart, const int *d_leaf_npart);
-/* One chunk of the interaction list: ntask (sink, source) leaf-id pairs. */
+/* One chunk of the interaction list: ntask (sink, source) leaf-id pairs.
+ * Host arrays (here and in p2p_pass_begin) are copied asynchronously: arrays
+ * in page-locked memory must stay unchanged until p2p_pass_end; pageable
+ * arrays may be reused once the call returns (the CUDA runtime stages a
+ * pageable source before cudaMemcpyAsync returns). */
 int p2p_pass_submit(p2p_session *s, int64_t ntask, const int *task_t, const int *task_s);
 int p2p_pass_submit_device(p2p_session *s, int64_t ntask, const int *d_task_t, const int *d_task_s);
 /* Completion barrier; *gpu_seconds (nullable) = device time from begin to
@@ -203,8 +207,9 @@ int p2p_session_last_kernel_ms(p2p_session *s, float *ms);
  * For callers that cannot have a library call cudaMalloc / cudaFree while
  * they run: codes that reserve nearly all device memory for their own pool
  * at start-up, processes held to a fixed device-memory quota on a shared GPU,
- * and pipelines that overlap host work with the GPU (cudaFree synchronises
- * the device). The pass's scratch is one file-scope __device__ array of
+ * and codes that keep other work running on their own streams (cudaFree
+ * synchronises the whole device; this call waits for its own stream only).
+ * The pass's scratch is one file-scope __device__ array of
  * P2P_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * the process exits; nothing else is allocated (no cudaMalloc / cudaFree, no
  * allocating library call, no session).
@@ -214,7 +219,12 @@ int p2p_session_last_kernel_ms(p2p_session *s, float *ms);
  * SoA), which is overwritten with the result. Equal masses (params->mass).
  * Forms: P2P_FORM_SPLIT (packed source-lane kernel) or P2P_FORM_PLAIN_FP64.
  * The pass is queued on `stream` (a cudaStream_t, 0 for the default stream)
- * and the call returns when it has finished there.
+ * and the call blocks the calling host thread until the pass has finished
+ * on that stream (it reads the pass's status word there); other streams and
+ * the rest of the device are not synchronised. The numeric fields of params
+ * are checked as p2p_session_set_params checks them; warps_per_block,
+ * blocks_per_sm and kernel_variant are ignored (the split form always runs
+ * the packed source-lane kernel, 4 warps per block, as many blocks as fit).
  *
  * Limit: the scratch needed, about 16*npart (split form only) + 48*nleaf +
  * 4*ntask bytes plus 256-byte alignment of each piece, must fit in

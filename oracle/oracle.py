@@ -215,3 +215,32 @@ class RefWalk:
             self.L.ref_record_copy(_p(tt), _p(ts), _p(ce))
             out.update(task_t=tt, task_s=ts, chunk_end=ce)
         return out
+
+
+def ref_pack_run(libname, pos, leaf_ipart, leaf_npart, leaf_base, split_radius, soften, mass, packs):
+    """The drop-in's multi-pack entry p2ppack_compute_gpu driven as the
+    reference's load-balanced walk calls it (oracle/ref_pack_harness.c).
+    packs: list of dicts with task_t, task_s (absolute leaf ids, i.e. 0-based
+    id + leaf_base), ileaf, nleaf, ipart, npart. Returns (acc (3, npart),
+    kernel seconds)."""
+    L = ctypes.CDLL(os.path.join(REF_DIR, libname), mode=ctypes.RTLD_LOCAL)
+    f = L.ref_pack_run
+    f.restype = ctypes.c_int
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = pos.shape[1]
+    ip = np.ascontiguousarray(leaf_ipart, np.int32)
+    npt = np.ascontiguousarray(leaf_npart, np.int32)
+    col = lambda k: np.ascontiguousarray([p[k] for p in packs], np.int32)  # noqa: E731
+    ntask = np.ascontiguousarray([len(p["task_t"]) for p in packs], np.int32)
+    tt = np.ascontiguousarray(np.concatenate([p["task_t"] for p in packs]), np.int32)
+    ts = np.ascontiguousarray(np.concatenate([p["task_s"] for p in packs]), np.int32)
+    cols = [col(k) for k in ("ileaf", "nleaf", "ipart", "npart")]
+    acc = np.zeros((3, n))
+    ksec = ctypes.c_double(0.0)
+    f.argtypes = ([ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int] + [ctypes.c_double] * 3 +
+                  [ctypes.c_int] + [_vp] * 9)
+    st = f(n, _p(pos), ip.shape[0], _p(ip), _p(npt), leaf_base, split_radius, soften, mass, len(packs),
+           _p(ntask), *[_p(c) for c in cols], _p(tt), _p(ts), _p(acc), ctypes.addressof(ksec))
+    if st != 0:
+        raise RuntimeError("pack harness failed")
+    return acc, ksec.value

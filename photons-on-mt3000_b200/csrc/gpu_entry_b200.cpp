@@ -11,7 +11,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <vector>
 
 extern "C" {
 #include "photoNs.h"
@@ -26,6 +25,34 @@ long long g_tot_tasks = 0;
 bool g_pass_open = false;
 double *g_out = nullptr;  // h_part_buf of the reference
 int g_out_n = 0;
+
+void check(const char *where, int status);
+
+// Page-locked staging the module owns (grow-only, freed by devfree): the
+// packed positions and leaf table of the open pass, and the rebased lists
+// of p2ppack_compute_gpu. Copies from them are asynchronous, so they stay
+// untouched until the pass has ended (get_last_kntime) or the next begins.
+struct Pinned {
+    void *p = nullptr;
+    size_t cap = 0;
+    void *get(size_t bytes) {
+        if (bytes > cap) {
+            if (p) p2p_host_free(p);
+            p = nullptr;
+            cap = 0;
+            const size_t want = bytes + bytes / 8;
+            check("p2p_host_alloc", p2p_host_alloc(want, &p));
+            cap = want;
+        }
+        return p;
+    }
+    void release() {
+        if (p) p2p_host_free(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+Pinned g_pin_pos, g_pin_leaf, g_pin_tasks;
 
 [[noreturn]] void die(const char *where, int status) {
     // checkDevErrors, src/gpu_func.impl.h:70-86
@@ -90,7 +117,7 @@ void begin_pass() {
     set_pass_params();
     const int n = NPART;
     const int nleaf = last_leaf - first_leaf;
-    std::vector<double> pos(3 * (size_t)n);
+    double *pos = (double *)g_pin_pos.get(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
     // (the reference packs on one thread; the iterations are independent)
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
@@ -102,12 +129,13 @@ void begin_pass() {
 #endif
         }
     }
-    std::vector<int> ip(nleaf), np(nleaf);
+    int *ip = (int *)g_pin_leaf.get(sizeof(int) * 2 * (size_t)(nleaf > 0 ? nleaf : 1));
+    int *np = ip + nleaf;
     for (int l = 0; l < nleaf; ++l) {
         ip[l] = leaf[l + first_leaf].ipart;
         np[l] = leaf[l + first_leaf].npart;
     }
-    check("p2p_pass_begin", p2p_pass_begin(g_sess, n, pos.data(), nullptr, nleaf, ip.data(), np.data()));
+    check("p2p_pass_begin", p2p_pass_begin(g_sess, n, pos, nullptr, nleaf, ip, np));
     g_pass_open = true;
 }
 
@@ -148,18 +176,32 @@ void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time)
     return NULL;
 }
 
+// Every pack of the pass on the one device (the reference spreads packs over
+// devices and gives each its own leaf and particle slices, src/gpu_entry.cu:211-386,
+// src/gpu_func.impl.h:588-618): here the whole local tree is resident, so each
+// pack's list, rebased to 0-based leaf ids, is one submit of the same pass.
+// The reference rebases the caller's arrays in place by the pack's first leaf
+// (devMemcpyHD_task, src/gpu_func.impl.h:704-713) and the caller does not
+// read them again; this copy leaves them as they are.
 void *p2ppack_compute_gpu(P2PPack *packs, int npack) {
     if (npack == 0) return NULL;
     begin_pass();
+    size_t total = 0;
+    for (int n = 0; n < npack; ++n) total += (size_t)(packs[n].ntask > 0 ? packs[n].ntask : 0);
+    int *buf = (int *)g_pin_tasks.get(sizeof(int) * 2 * (total > 0 ? total : 1));
+    size_t off = 0;
     for (int n = 0; n < npack; ++n) {
-        if (packs[n].ntask == 0) continue;
+        if (packs[n].ntask <= 0) continue;
         packs[n].rankid = 0;
-        std::vector<int> t(packs[n].ntask), s(packs[n].ntask);
-        for (int j = 0; j < packs[n].ntask; ++j) {
+        const int m = packs[n].ntask;
+        int *t = buf + 2 * off, *s = t + m;
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < m; ++j) {
             t[j] = packs[n].task_t[j] - first_leaf;
             s[j] = packs[n].task_s[j] - first_leaf;
         }
-        check("p2p_pass_submit", p2p_pass_submit(g_sess, packs[n].ntask, t.data(), s.data()));
+        check("p2p_pass_submit", p2p_pass_submit(g_sess, m, t, s));
+        off += (size_t)m;
     }
     return NULL;
 }
@@ -199,8 +241,12 @@ void hostfree_out(void) {
     g_out_n = 0;
 }
 
-// D2H of the result, then acc[d][j] += buf for the particles of each pack
-// (updateAcc_fromHostBuff, src/gpu_func.impl.h:644-681).
+// D2H of the result, then acc[d][j] += buf over the particles of the packs
+// (updateAcc_fromHostBuff, src/gpu_func.impl.h:644-681). The reference keeps
+// one result slice per pack and adds each over its pack's particle range;
+// here the pass leaves one total per particle, so it is added once for every
+// particle that some pack covers (pack ranges may overlap: the walk's
+// inter-subtree pack spans the others, src/fmm_LB.c:25-49,215-228).
 void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
     if (!g_sess) return;
     bool any = false;
@@ -212,11 +258,35 @@ void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
     }
     check("p2p_pass_result", p2p_pass_result(g_sess, g_out));
     const int n = NPART;
+    // the union of the packs' particle ranges, as sorted disjoint intervals
+    int *lo = (int *)malloc(sizeof(int) * 2 * (size_t)(npack > 0 ? npack : 1));
+    int *hi = lo + npack;
+    int nr = 0;
     for (int p = 0; p < npack; ++p) {
-        if (packs[p].ntask == 0) continue;
+        if (packs[p].ntask == 0 || packs[p].npart <= 0) continue;
+        int a = packs[p].ipart, b = packs[p].ipart + packs[p].npart, k = nr++;
+        while (k > 0 && lo[k - 1] > a) {  // insertion by start
+            lo[k] = lo[k - 1];
+            hi[k] = hi[k - 1];
+            --k;
+        }
+        lo[k] = a;
+        hi[k] = b;
+    }
+    int m = 0;
+    for (int k = 0; k < nr; ++k) {
+        if (m > 0 && lo[k] <= hi[m - 1]) {
+            if (hi[k] > hi[m - 1]) hi[m - 1] = hi[k];
+        } else {
+            lo[m] = lo[k];
+            hi[m] = hi[k];
+            ++m;
+        }
+    }
+    for (int r = 0; r < m; ++r) {
+        const int a = lo[r] < 0 ? 0 : lo[r], b = hi[r] > n ? n : hi[r];
 #pragma omp parallel for schedule(static)
-        for (int i = 0; i < packs[p].npart; ++i) {
-            const int j = packs[p].ipart + i;
+        for (int j = a; j < b; ++j) {
             if (active_level == -1 || (active_level && part[j].act == active_level)) {
                 acc[0][j] += g_out[j];
                 acc[1][j] += g_out[(size_t)n + j];
@@ -224,11 +294,15 @@ void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
             }
         }
     }
+    free(lo);
 }
 
 void devfree(void) {
     if (g_sess) p2p_session_destroy(g_sess);
     g_sess = nullptr;
+    g_pin_pos.release();
+    g_pin_leaf.release();
+    g_pin_tasks.release();
     g_pass_open = false;
     g_call_cnt = 0;
     g_tot_tasks = 0;

@@ -4,8 +4,9 @@
 // cudaFree while they run. Examples are a simulation that reserves nearly all
 // of the GPU's memory for its own pool at start-up (a library allocation
 // then fails, or fragments the pool), a process held to a fixed device-memory
-// quota on a shared GPU, and a pipeline that overlaps host work with the
-// GPU pass (cudaFree synchronises the device and would stall it). For them
+// quota on a shared GPU, and a code that runs other work on its own streams
+// meanwhile (cudaFree synchronises the whole device and would stall those
+// streams; this call waits for its own stream only). For them
 // the scratch this pass needs lives in one file-scope __device__ array of a
 // fixed size, P2P_NOALLOC_SCRATCH_BYTES, that every GPU loading the library
 // holds until the process exits. The caller passes inputs and the output.
@@ -15,6 +16,7 @@
 // static array and launches them on the caller's stream.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -122,31 +124,57 @@ int grid_cap(int64_t n, int threads, int cap) {
     return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+// The persistent pair kernel's launch: with blocks == 0 it only resolves the
+// grid (resident blocks per SM times SMs) into *blocks; otherwise it launches.
 template <class K>
 int launch_persistent(K kernel, int sms, int warps, size_t smem, cudaStream_t st,
-                      const PairArgs &a, int stage) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, warps * 32, smem) != cudaSuccess ||
-        per_sm < 1) {
-        cudaGetLastError();
-        return P2P_ERR_ARG;
+                      const PairArgs &a, int stage, int *blocks) {
+    if (*blocks == 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, warps * 32, smem) != cudaSuccess ||
+            per_sm < 1) {
+            cudaGetLastError();
+            return P2P_ERR_ARG;
+        }
+        *blocks = per_sm * sms;
+        return P2P_OK;
     }
-    kernel<<<per_sm * sms, warps * 32, smem, st>>>(a, stage);
+    kernel<<<*blocks, warps * 32, smem, st>>>(a, stage);
     return cudaGetLastError() == cudaSuccess ? P2P_OK : P2P_ERR_CUDA;
 }
 
 template <int SOFT>
 int launch_split(int nc, int sms, int warps, size_t smem, cudaStream_t st, const PairArgs &a,
-                 int stage) {
+                 int stage, int *blocks) {
     switch (nc) {
-        case 9: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 9>, sms, warps, smem, st, a, stage);
-        case 11: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 11>, sms, warps, smem, st, a, stage);
-        case 13: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 13>, sms, warps, smem, st, a, stage);
-        case 15: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 15>, sms, warps, smem, st, a, stage);
-        case 17: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 17>, sms, warps, smem, st, a, stage);
-        case 21: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 21>, sms, warps, smem, st, a, stage);
+        case 9: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 9>, sms, warps, smem, st, a, stage, blocks);
+        case 11: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 11>, sms, warps, smem, st, a, stage, blocks);
+        case 13: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 13>, sms, warps, smem, st, a, stage, blocks);
+        case 15: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 15>, sms, warps, smem, st, a, stage, blocks);
+        case 17: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 17>, sms, warps, smem, st, a, stage, blocks);
+        case 21: return launch_persistent(pair_split_src2_kernel<SOFT, false, ACC_F64, 21>, sms, warps, smem, st, a, stage, blocks);
         default: return P2P_ERR_STATE;
     }
+}
+
+// The pair kernel of these parameters (blocks == 0: resolve the grid only).
+int launch_pair_kernel(bool fp32, const p2p_params &p, int nc, int sms, int warps, size_t smem, cudaStream_t s,
+                       const PairArgs &a, int stage, int *blocks) {
+    if (fp32)
+        return p.soft_mode == P2P_SOFT_CLAMP ? launch_split<SOFT_CLAMP>(nc, sms, warps, smem, s, a, stage, blocks)
+                                             : launch_split<SOFT_PLUMMER>(nc, sms, warps, smem, s, a, stage, blocks);
+    return p.soft_mode == P2P_SOFT_CLAMP
+               ? launch_persistent(pair_plain_kernel<SOFT_CLAMP, false>, sms, warps, smem, s, a, stage, blocks)
+               : launch_persistent(pair_plain_kernel<SOFT_PLUMMER, false>, sms, warps, smem, s, a, stage, blocks);
+}
+
+// An error after work was queued: the call still returns only once that work
+// (which writes the shared scratch) has finished on the stream.
+int fail_after_queue(cudaStream_t s, int status) {
+    cudaGetLastError();
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    return status;
 }
 
 }  // namespace
@@ -163,7 +191,11 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     const p2p_params &p = *params;
     if (p.form != P2P_FORM_SPLIT && p.form != P2P_FORM_PLAIN_FP64) return P2P_ERR_ARG;
     if (p.soft_mode != P2P_SOFT_CLAMP && p.soft_mode != P2P_SOFT_PLUMMER) return P2P_ERR_ARG;
-    if (!(p.soften > 0.0) || !(p.split_radius > 0.0)) return P2P_ERR_ARG;
+    // the session's checks of the numeric fields (p2p_session_set_params)
+    if (!(p.soften > 0.0) || !std::isfinite(p.soften)) return P2P_ERR_ARG;
+    if (!(p.split_radius > 0.0) || !std::isfinite(p.split_radius)) return P2P_ERR_ARG;
+    if (!std::isfinite(p.x_cut) || !std::isfinite(p.mass)) return P2P_ERR_ARG;
+    if (!(p.poly_tol >= 0.0) || !std::isfinite(p.poly_tol)) return P2P_ERR_ARG;
     if (npart < 0 || nleaf < 0 || ntask < 0) return P2P_ERR_ARG;
     if ((npart > 0 && (!d_pos || !d_acc)) || (nleaf > 0 && (!d_leaf_ipart || !d_leaf_npart)) ||
         (ntask > 0 && (!d_task_t || !d_task_s)))
@@ -201,6 +233,15 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     }
 
     cudaStream_t s = (cudaStream_t)stream;
+    // the pair kernel's grid, and that the fit has an instantiated degree,
+    // before anything is queued
+    int blocks = 0;
+    {
+        PairArgs probe;
+        memset(&probe, 0, sizeof(probe));
+        st = launch_pair_kernel(fp32, p, fit.ncoef_kernel, sms, warps, smem, s, probe, stage, &blocks);
+        if (st != P2P_OK) return st;
+    }
     LeafMeta *meta = (LeafMeta *)(base + L.meta);
     float4 *pos4 = (float4 *)(base + L.pos4);
     int *counts = (int *)(base + L.counts);
@@ -219,13 +260,10 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
         ok = ok && cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nleaf, s) == cudaSuccess;
         ok = ok && cudaMemsetAsync(fill, 0, sizeof(int) * (size_t)nleaf, s) == cudaSuccess;
     }
-    if (!ok) {
-        cudaGetLastError();
-        return P2P_ERR_CUDA;
-    }
+    if (!ok) return fail_after_queue(s, P2P_ERR_CUDA);
     if (nleaf == 0 || ntask == 0) {
         // nothing to sum: the zeroed output is the result
-        return cudaStreamSynchronize(s) == cudaSuccess ? P2P_OK : P2P_ERR_CUDA;
+        return cudaStreamSynchronize(s) == cudaSuccess ? P2P_OK : fail_after_queue(s, P2P_ERR_CUDA);
     }
     const double c = 0.5 / p.split_radius;
     const int threads = 256;
@@ -247,7 +285,7 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     csr_sort_rows_warp_kernel<<<grid_cap(nleaf, 4, sms * 8), 128, 0, s>>>(row_off, nleaf, row_src);
     csr_sort_rows_block_kernel<<<grid_cap(nleaf, 1, sms * 2), kSortBlockThreads, 0, s>>>(row_off, nleaf, row_src);
     csr_sort_rows_global_kernel<<<grid_cap(nleaf, 1, sms), kSortBlockThreads, 0, s>>>(row_off, nleaf, row_src);
-    if (cudaGetLastError() != cudaSuccess) return P2P_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return fail_after_queue(s, P2P_ERR_CUDA);
 
     PairArgs a;
     memset(&a, 0, sizeof(a));
@@ -262,24 +300,13 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     a.npart = npart;
     a.nleaf = nleaf;
     fill_pass_scalars(a, p, fit, false);
-    if (fp32) {
-        st = p.soft_mode == P2P_SOFT_CLAMP
-                 ? launch_split<SOFT_CLAMP>(fit.ncoef_kernel, sms, warps, smem, s, a, stage)
-                 : launch_split<SOFT_PLUMMER>(fit.ncoef_kernel, sms, warps, smem, s, a, stage);
-    } else {
-        st = p.soft_mode == P2P_SOFT_CLAMP
-                 ? launch_persistent(pair_plain_kernel<SOFT_CLAMP, false>, sms, warps, smem, s, a, stage)
-                 : launch_persistent(pair_plain_kernel<SOFT_PLUMMER, false>, sms, warps, smem, s, a, stage);
-    }
-    if (st != P2P_OK) return st;
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
-        cudaGetLastError();
-        return P2P_ERR_CUDA;
-    }
+    st = launch_pair_kernel(fp32, p, fit.ncoef_kernel, sms, warps, smem, s, a, stage, &blocks);
+    if (st != P2P_OK) return fail_after_queue(s, st);
+    // the status word read on the caller's stream, behind the pass; the call
+    // returns once that stream has reached it
     int flags = 0;
-    if (cudaMemcpy(&flags, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        cudaGetLastError();
-        return P2P_ERR_CUDA;
-    }
+    if (cudaMemcpyAsync(&flags, status, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail_after_queue(s, P2P_ERR_CUDA);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return fail_after_queue(s, P2P_ERR_CUDA);
     return flags ? P2P_ERR_RANGE : P2P_OK;
 }

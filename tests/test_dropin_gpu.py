@@ -48,3 +48,51 @@ def test_reference_fmm_task_through_dropin(gpu, case, variant, max_tol, rms_tol)
     assert out["kernel_seconds"] > 0
     rms, mx = rel_err(out["acc"], ref, local)
     assert mx <= max_tol and rms <= rms_tol, (rms, mx)
+
+
+def lb_packs(tl, nsub, leaf_base):
+    """Packs as the reference's load-balanced walk makes them
+    (add_one_p2ppack, src/fmm_LB.c:25-49): the entries whose sink and source
+    both lie in one of nsub contiguous leaf ranges (subtrees) form that
+    range's pack, the remaining entries one last inter-subtree pack; each
+    pack's leaf and particle range spans its smallest to largest leaf id, so
+    the inter-subtree pack overlaps the others."""
+    L = tl.nleaf
+    cut = np.linspace(0, L, nsub + 1).astype(np.int64)
+    sub_t = np.searchsorted(cut, tl.task_t, side="right") - 1
+    sub_s = np.searchsorted(cut, tl.task_s, side="right") - 1
+    groups = [np.nonzero((sub_t == k) & (sub_s == k))[0] for k in range(nsub)]
+    groups.append(np.nonzero(sub_t != sub_s)[0])
+    packs = []
+    for g in groups:
+        if g.size == 0:
+            continue
+        t, s = tl.task_t[g], tl.task_s[g]
+        lo, hi = int(min(t.min(), s.min())), int(max(t.max(), s.max()))
+        packs.append(dict(task_t=t + leaf_base, task_s=s + leaf_base, ileaf=lo + leaf_base, nleaf=hi - lo + 1,
+                          ipart=int(tl.leaf_ipart[lo]),
+                          npart=int(tl.leaf_ipart[hi] - tl.leaf_ipart[lo] + tl.leaf_npart[hi])))
+    return packs
+
+
+@pytest.mark.parametrize("variant,max_tol,rms_tol", [("dp", 1e-12, 1e-12), ("sp", 1e-3, 1e-5)])
+def test_multi_pack_entry_point(gpu, variant, max_tol, rms_tol):
+    """p2ppack_compute_gpu with four subtree packs and an overlapping
+    inter-subtree pack (the reference's INTRA_LB protocol, src/fmm.c:1245-1250,
+    src/gpu_entry.cu:211-386), then get_last_kntime + devMemcpyDH_updateAcc:
+    every particle receives its pairs once, as the oracle computes them on
+    the whole list."""
+    cfg = W.ref_dropin_config(32, 64, 32)
+    pos = W.lattice_gaussian(32, 0.2, W.rng(1))
+    tl = W.prepare(pos, cfg)
+    mass = 1.0 / pos.shape[1]
+    leaf_base = 5  # a biased leaf pointer, as PhotoNs' first_leaf
+    packs = lb_packs(tl, 4, leaf_base)
+    assert len(packs) == 5 and sum(len(p["task_t"]) for p in packs) == tl.ntask
+    ref, _ = O.p2p_lists(O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass), tl.pos,
+                         tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+    got, ksec = O.ref_pack_run(f"libref_dropin_{variant}.so", tl.pos, tl.leaf_ipart, tl.leaf_npart, leaf_base,
+                               cfg.split_radius, cfg.eps, mass, packs)
+    assert ksec > 0
+    rms, mx = rel_err(got, ref, tl.tag == 1)
+    assert mx <= max_tol and rms <= rms_tol, (rms, mx)

@@ -2,8 +2,10 @@
 
 It is meant for host codes that cannot have a library call cudaMalloc or
 cudaFree while they run (a simulation that reserves the GPU's memory for its
-own pool, a process under a fixed device-memory quota, a pipeline that must
-not be stalled by cudaFree's device synchronisation). Its scratch is a fixed
+own pool, a process under a fixed device-memory quota, a code whose other
+streams must not be stalled by cudaFree's device-wide synchronisation; the
+call itself blocks its host thread until its own stream has finished the
+pass). Its scratch is a fixed
 static device array, so two calls in a row must give the same forces as the
 session entry point (p2p_pass_run_device), within the same tolerances the
 parity tests use. This file is collected last so that a run stopping at the
