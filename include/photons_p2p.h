@@ -74,7 +74,8 @@ typedef struct {
 } p2p_params;
 
 /* Lane mappings of the FP32 pair kernel. */
-#define P2P_VARIANT_AUTO 0            /* the fastest mapping (P2P_VARIANT_SOURCE_LANES_X2) */
+#define P2P_VARIANT_AUTO 0            /* the session's fastest mapping (P2P_VARIANT_SINK_REGS);
+                                         the ensemble server's P2P_VARIANT_SOURCE_LANES_X2 */
 #define P2P_VARIANT_SINK_LANES 1      /* one lane per sink particle, sources broadcast */
 #define P2P_VARIANT_SOURCE_LANES 2    /* one lane per staged source, sinks broadcast */
 #define P2P_VARIANT_SOURCE_LANES_X2 3 /* source lanes, two sinks per packed f32x2 instruction,
@@ -187,6 +188,37 @@ typedef struct p2p_walk_tree {
  * sink's pending pairs exceed the walk's fixed stack. */
 int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *tree, double cutoff, double open_angle,
                          int64_t *ntask);
+/* ---- Device kd-tree (no counterpart in the reference's GPU code) --------
+ * Builds on the GPU the tree PhotoNs builds on the host before its walk
+ * (build_kdtree / center_kdtree, src/fmm.c:69-122,231-327; leaf.active,
+ * src/fmm.c:1226-1236): the same mean splits (axis depth % 3, sampled mean
+ * summed in slot order, the same in-place partition), the same particle
+ * order, pre-order node and leaf numbering and boxes; the root box is
+ * particle_combine's float-rounded bounds widened by 1e-6 boxsize
+ * (src/gravity.c:69-121). d_pos: 3*npart doubles (SoA, device), d_tag
+ * (nullable: all local): npart ints, 1 for local particles. Runs on the
+ * session's stream and returns when the tree is complete. The tree owns its
+ * device arrays until p2p_dtree_free. P2P_ERR_CAPACITY when the tree needs
+ * more than min(npart + 1, 8 npart / maxleaf + 1024) nodes or leaves. */
+typedef struct p2p_dtree p2p_dtree;
+int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, const int *d_tag, int maxleaf,
+                    double boxsize, p2p_dtree **out);
+int p2p_dtree_free(p2p_dtree *t);
+/* Sizes and the build's device time (ms, CUDA events; nullable outputs). */
+int p2p_dtree_counts(const p2p_dtree *t, int *npart, int *nleaf, int *nnode, float *build_ms);
+/* Device arrays owned by the tree (nullable outputs): positions in tree
+ * order (3*npart SoA), perm[slot] = input index, leaf particle ranges: the
+ * inputs of p2p_pass_begin_device. */
+int p2p_dtree_device_arrays(const p2p_dtree *t, const double **d_pos, const int **d_perm,
+                            const int **d_leaf_ipart, const int **d_leaf_npart);
+/* The node and leaf tables as the walk reads them (p2p_pass_submit_walk). */
+int p2p_dtree_walk_tree(const p2p_dtree *t, p2p_walk_tree *tree);
+/* Host copies of the tree (every output nullable; sizes from p2p_dtree_counts;
+ * centres and widths AoS, 3 per entry; son 2 per node). */
+int p2p_dtree_download(const p2p_dtree *t, double *pos, int *perm, int *leaf_ipart, int *leaf_npart,
+                       int *leaf_active, double *leaf_center, double *leaf_width, int *son, int *node_first,
+                       double *node_center, double *node_width);
+
 /* Host copy of the CSR rows of the last submitted chunk or walk (row_off:
  * nleaf+1 entries; row_src (nullable: rows not copied): row_off[nleaf]
  * entries). Call after p2p_pass_end. */

@@ -184,15 +184,17 @@ bool source_lanes(const p2p_params &p) {
 
 bool packed_lanes(const p2p_params &p) {
     return p.form != P2P_FORM_PLAIN_FP64 &&
-           (p.kernel_variant == P2P_VARIANT_AUTO || p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2 ||
+           (p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2 ||
             p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16);
 }
 
 // Whether the pair kernel counts the pairs it evaluates on the device (the
 // sink-register kernel, which also drops single source particles).
-bool counts_evaluated(const p2p_params &p) {
-    return is_fp32_form(p.form) && p.kernel_variant == P2P_VARIANT_SINK_REGS;
+bool sink_regs(const p2p_params &p) {
+    return is_fp32_form(p.form) &&
+           (p.kernel_variant == P2P_VARIANT_SINK_REGS || p.kernel_variant == P2P_VARIANT_AUTO);
 }
+bool counts_evaluated(const p2p_params &p) { return sink_regs(p); }
 
 int default_stage(const p2p_params &p) {
     return p.stage_sources ? p.stage_sources : (p.form == P2P_FORM_PLAIN_FP64 ? 128 : 256);
@@ -219,7 +221,7 @@ int launch_pair(p2p_session *s, const PairArgs &a) {
         r = launch_pair_plain(L, a);
     else if (p.kernel_variant == P2P_VARIANT_SINK_LANES_X2)
         r = launch_pair_sink_lanes_x2(L, a);
-    else if (p.kernel_variant == P2P_VARIANT_SINK_REGS)
+    else if (sink_regs(p))
         r = launch_pair_sink_regs(L, a);
     else if (packed_lanes(p))
         r = launch_pair_source_lanes_x2(L, a);
@@ -416,6 +418,7 @@ int report_error(int status, const char *msg) {
 int check_params(const p2p_params *p) { return validate_params(p); }
 void count_launches(int n) { g_launches += n; }
 cudaError_t allow_large_smem() { return allow_smem_all(); }
+int session_device(const p2p_session *s) { return s ? s->device : 0; }
 }  // namespace p2p
 
 // ------------------------------------------------------------------ ABI ---

@@ -15,4 +15,6 @@ int check_params(const p2p_params *p);
 void count_launches(int n);
 // Opts every pair kernel into large dynamic shared memory on the current device.
 cudaError_t allow_large_smem();
+// The CUDA device of a session.
+int session_device(const p2p_session *s);
 }  // namespace p2p

@@ -145,6 +145,14 @@ SIGNATURES = {
     "p2p_server_query": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_d)]),
     "p2p_server_drain": (_i, [_vp]),
     "p2p_server_get_stats": (_i, [_vp, ctypes.POINTER(ServerStats)]),
+    "p2p_dtree_build": (_i, [_vp, _i, _vp, _vp, _i, _d, ctypes.POINTER(_vp)]),
+    "p2p_dtree_free": (_i, [_vp]),
+    "p2p_dtree_counts": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
+                              ctypes.POINTER(ctypes.c_float)]),
+    "p2p_dtree_device_arrays": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                     ctypes.POINTER(_vp)]),
+    "p2p_dtree_walk_tree": (_i, [_vp, ctypes.POINTER(WalkTree)]),
+    "p2p_dtree_download": (_i, [_vp] + [_vp] * 11),
     "p2p_host_alloc": (_i, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "p2p_host_free": (_i, [_vp]),
 }

@@ -218,3 +218,64 @@ class DeviceWalkTree:
         self.struct = abi.WalkTree(son.shape[0], tree.nleaf, t[0].data_ptr(), t[1].data_ptr(),
                                    t[2].data_ptr(), t[3].data_ptr(), t[4].data_ptr(), t[5].data_ptr(),
                                    t[6].data_ptr())
+
+
+class DeviceTree:
+    """The kd-tree built on the GPU (p2p_dtree_build): the tree PhotoNs builds
+    on the host before its walk (src/fmm.c:69-327), equal node for node.
+    pos_dev: torch float64 tensor (3, n) on the session's device (SoA rows);
+    tag_dev: torch int32 (n,) or None (all local)."""
+
+    def __init__(self, session, pos_dev, tag_dev, maxleaf, boxsize):
+        self.lib = session.lib
+        self.session = session
+        n = int(pos_dev.shape[-1])
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.p2p_dtree_build(session.h, n, pos_dev.data_ptr(),
+                                                  tag_dev.data_ptr() if tag_dev is not None else None,
+                                                  maxleaf, boxsize, ctypes.byref(h)))
+        self.h = h
+        a, b, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(self.lib, self.lib.p2p_dtree_counts(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
+                                                   ctypes.byref(ms)))
+        self.npart, self.nleaf, self.nnode, self.build_ms = a.value, b.value, c.value, ms.value
+        self.struct = abi.WalkTree()
+        _check(self.lib, self.lib.p2p_dtree_walk_tree(self.h, ctypes.byref(self.struct)))
+
+    def device_arrays(self):
+        """(d_pos, d_perm, d_leaf_ipart, d_leaf_npart) device pointers (ints)."""
+        p = [ctypes.c_void_p() for _ in range(4)]
+        _check(self.lib, self.lib.p2p_dtree_device_arrays(self.h, *[ctypes.byref(x) for x in p]))
+        return tuple(x.value for x in p)
+
+    def download(self):
+        """Host copies: dict of pos (3, n), perm, leaf_ipart, leaf_npart,
+        leaf_active, leaf_center (nleaf, 3), leaf_width, son (nnode, 2),
+        node_first, node_center (nnode, 3), node_width."""
+        n, nl, nn = self.npart, self.nleaf, self.nnode
+        out = dict(pos=np.empty((3, n)), perm=np.empty(n, np.int32), leaf_ipart=np.empty(nl, np.int32),
+                   leaf_npart=np.empty(nl, np.int32), leaf_active=np.empty(nl, np.int32),
+                   leaf_center=np.empty((nl, 3)), leaf_width=np.empty((nl, 3)), son=np.empty((nn, 2), np.int32),
+                   node_first=np.empty(nn, np.int32), node_center=np.empty((nn, 3)), node_width=np.empty((nn, 3)))
+        keys = ["pos", "perm", "leaf_ipart", "leaf_npart", "leaf_active", "leaf_center", "leaf_width", "son",
+                "node_first", "node_center", "node_width"]
+        _check(self.lib, self.lib.p2p_dtree_download(self.h, *[out[k].ctypes.data_as(ctypes.c_void_p)
+                                                               for k in keys]))
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.p2p_dtree_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

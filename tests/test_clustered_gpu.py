@@ -56,7 +56,7 @@ def test_plain_vs_direct(gpu, clustered):
     assert mx <= 1e-10, (rms, mx)
 
 
-@pytest.mark.parametrize("variant", [abi.VARIANT_AUTO, abi.VARIANT_SOURCE_LANES_X2_S16,
+@pytest.mark.parametrize("variant", [abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SOURCE_LANES_X2_S16,
                                      abi.VARIANT_SINK_LANES_X2, abi.VARIANT_SINK_REGS])
 def test_split_vs_direct(gpu, clustered, variant):
     cfg, tl, mass, rows, ref = clustered
@@ -66,7 +66,7 @@ def test_split_vs_direct(gpu, clustered, variant):
     assert 0 < evaluated < tl.pair_count()
 
 
-@pytest.mark.parametrize("variant", [abi.VARIANT_AUTO, abi.VARIANT_SINK_REGS])
+@pytest.mark.parametrize("variant", [abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SINK_REGS])
 def test_kahan_vs_direct(gpu, clustered, variant):
     cfg, tl, mass, rows, ref = clustered
     acc, _ = run(cfg, tl, mass, abi.FORM_KAHAN_FP32, variant)
