@@ -221,13 +221,99 @@ def walk_leg(sess, cfg, raw_pos, tl, dev, d_pos, d_ip, d_np, pairs, steps=3):
                 kern.append(sess.last_kernel_ms())
         launches = (kernel_launch_count() - l0) // (steps + 1)
         walk_pairs = sess.pair_count()
+        host_perm, host_ip = tree.perm.copy(), tree.leaf_ipart.copy()
     pass_s, kern_ms = float(np.mean(times)), float(np.mean(kern))
-    return {"host_tree_s": round(tree_s, 2), "host_walk_s": round(host_walk_s, 2),
-            "host_walk_cores": L.num_threads(), "entries": int(ntask),
-            "entries_equal_host": bool(ntask == ntask_host), "pairs_equal": bool(walk_pairs == pairs),
-            "pass_ms": 1e3 * pass_s, "pair_kernel_ms": kern_ms,
-            "walk_and_prep_ms": 1e3 * pass_s - kern_ms, "pairs_per_s": pairs / pass_s,
-            "gpu_launches_per_pass": int(launches)}
+    out = {"host_tree_s": round(tree_s, 2), "host_walk_s": round(host_walk_s, 2),
+           "host_walk_cores": L.num_threads(), "entries": int(ntask),
+           "entries_equal_host": bool(ntask == ntask_host), "pairs_equal": bool(walk_pairs == pairs),
+           "pass_ms": 1e3 * pass_s, "pair_kernel_ms": kern_ms,
+           "walk_and_prep_ms": 1e3 * pass_s - kern_ms, "pairs_per_s": pairs / pass_s,
+           "gpu_launches_per_pass": int(launches)}
+    out["device_tree"] = device_tree_leg(sess, cfg, allpos, tag, dev, host_perm, host_ip, pairs, steps)
+    return out
+
+
+def device_tree_leg(sess, cfg, allpos, tag, dev, host_perm, host_ip, pairs, steps=3):
+    """Tree, walk and pass all on the GPU from the particles (with ghosts) in
+    device memory: p2p_dtree_build (the reference's kd-tree, built on the
+    GPU), then p2p_pass_begin_device + p2p_pass_submit_walk on its arrays.
+    Times the tree build (CUDA events) and the whole sequence (wall clock
+    around the calls, which wait for the GPU)."""
+    import torch
+
+    from photons_p2p.p2p import DeviceTree
+
+    d_all = torch.from_numpy(np.ascontiguousarray(allpos)).to(dev)
+    d_tag = torch.from_numpy(np.ascontiguousarray(tag, dtype=np.int32)).to(dev)
+    torch.cuda.synchronize()
+    build_ms, total_s, equal = [], [], True
+    lib = sess.lib
+    for k in range(steps + 1):
+        t0 = time.perf_counter()
+        with DeviceTree(sess, d_all, d_tag, cfg.maxleaf, cfg.box) as t:
+            d_pos, _, d_ip, d_np = t.device_arrays()
+            if lib.p2p_pass_begin_device(sess.h, t.npart, d_pos, None, t.nleaf, d_ip, d_np):
+                raise RuntimeError(lib.p2p_last_error().decode())
+            sess.submit_walk(t, cfg.cutoff_radius, cfg.open_angle)
+            sess.end()
+            el = time.perf_counter() - t0
+            if k == 0:  # the first build is checked against the host tree
+                d = t.download()
+                equal = bool(np.array_equal(d["perm"], host_perm) and np.array_equal(d["leaf_ipart"], host_ip))
+                got_pairs = sess.pair_count()
+            else:
+                build_ms.append(t.build_ms)
+                total_s.append(el)
+    out = {"tree_ms": float(np.mean(build_ms)), "tree_walk_pass_ms": 1e3 * float(np.mean(total_s)),
+           "tree_equal_host": equal, "pairs_equal": bool(got_pairs == pairs),
+           "pairs_per_s": pairs / float(np.mean(total_s))}
+    out["e2e_particles"] = particles_e2e(sess, cfg, allpos, tag, dev, pairs, steps)
+    return out
+
+
+def particles_e2e(sess, cfg, allpos, tag, dev, pairs, steps=3):
+    """End to end from particles to forces through the C ABI: positions and
+    tags (with ghosts) from page-locked host memory to the device, the tree
+    (p2p_dtree_build), the list walk and the pass (p2p_pass_submit_walk), the
+    forces back to input order (p2p_dtree_unpermute) and to page-locked host
+    memory for the local particles; wall clock around it all, every step."""
+    import torch
+
+    from photons_p2p.p2p import DeviceTree
+
+    n = allpos.shape[1]
+    nlocal = int(np.count_nonzero(tag))
+    h_pos = torch.from_numpy(np.ascontiguousarray(allpos)).pin_memory()
+    h_tag = torch.from_numpy(np.ascontiguousarray(tag, dtype=np.int32)).pin_memory()
+    h_out = torch.empty((3, nlocal), dtype=torch.float64).pin_memory()
+    d_pos = torch.empty((3, n), dtype=torch.float64, device=dev)
+    d_tag = torch.empty(n, dtype=torch.int32, device=dev)
+    d_out = torch.empty((3, n), dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(sess.stream, device=dev)
+    lib = sess.lib
+    times = []
+    for k in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            d_pos.copy_(h_pos, non_blocking=True)
+            d_tag.copy_(h_tag, non_blocking=True)
+        with DeviceTree(sess, d_pos, d_tag, cfg.maxleaf, cfg.box) as t:
+            dp, _, dip, dnp = t.device_arrays()
+            if lib.p2p_pass_begin_device(sess.h, t.npart, dp, None, t.nleaf, dip, dnp):
+                raise RuntimeError(lib.p2p_last_error().decode())
+            sess.submit_walk(t, cfg.cutoff_radius, cfg.open_angle)
+            sess.end()
+            t.unpermute(sess.result_device(), d_out.data_ptr())
+            with torch.cuda.stream(stream):
+                h_out.copy_(d_out[:, :nlocal], non_blocking=True)
+            stream.synchronize()
+        if k:
+            times.append(time.perf_counter() - t0)
+    e = float(np.mean(times))
+    return {"value": pairs / e, "unit": "pairs/s", "ms": 1e3 * e,
+            "h2d_bytes_per_step": int(h_pos.numel() * 8 + h_tag.numel() * 4),
+            "d2h_bytes_per_step": int(h_out.numel() * 8)}
 
 
 def run_ours(args, rank, world, dist):

@@ -213,6 +213,10 @@ int p2p_dtree_device_arrays(const p2p_dtree *t, const double **d_pos, const int 
                             const int **d_leaf_ipart, const int **d_leaf_npart);
 /* The node and leaf tables as the walk reads them (p2p_pass_submit_walk). */
 int p2p_dtree_walk_tree(const p2p_dtree *t, p2p_walk_tree *tree);
+/* Reorders a per-particle SoA result (3*npart doubles, device) from tree
+ * order to the order of the build's input positions: d_out[d*npart +
+ * perm[i]] = d_in[d*npart + i]. Queued on the session's stream. */
+int p2p_dtree_unpermute(const p2p_dtree *t, p2p_session *s, const double *d_in, double *d_out);
 /* Host copies of the tree (every output nullable; sizes from p2p_dtree_counts;
  * centres and widths AoS, 3 per entry; son 2 per node). */
 int p2p_dtree_download(const p2p_dtree *t, double *pos, int *perm, int *leaf_ipart, int *leaf_npart,

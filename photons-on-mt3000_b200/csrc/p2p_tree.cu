@@ -182,7 +182,7 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
         TREE_CUDA(cudaMemcpyAsync(d_segs, segs.data(), sizeof(TreeSeg) * nseg, cudaMemcpyHostToDevice, st));
         TREE_CUDA(cudaMemcpyAsync(d_tile_seg, tile_seg.data(), sizeof(int) * ntile, cudaMemcpyHostToDevice, st));
         TREE_CUDA(cudaMemcpyAsync(d_tile_off, tile_off.data(), sizeof(int) * ntile, cudaMemcpyHostToDevice, st));
-        tree_seg_mean_kernel<<<grid(nseg, 128, 1 << 20), 128, 0, st>>>(d_segs, nseg, P, R);
+        tree_seg_mean_kernel<<<nseg, kTreeThreads, 0, st>>>(d_segs, P, R);
         tree_tile_count_kernel<<<ntile, kTreeThreads, 0, st>>>(d_segs, d_tile_seg, d_tile_off, P, d_tile_small);
         launches += 2;
         std::vector<int> tsmall(ntile), tpre(ntile);
@@ -353,6 +353,17 @@ P2P_API int p2p_dtree_walk_tree(const p2p_dtree *t, p2p_walk_tree *w) {
     w->leaf_center = t->leaf_center;
     w->leaf_width = t->leaf_width;
     w->leaf_active = t->leaf_active;
+    return P2P_OK;
+}
+
+P2P_API int p2p_dtree_unpermute(const p2p_dtree *t, p2p_session *s, const double *d_in, double *d_out) {
+    if (!t || !s || !d_in || !d_out) return report_error(P2P_ERR_ARG, "null argument");
+    if (d_in == d_out) return report_error(P2P_ERR_ARG, "unpermute needs distinct buffers");
+    TREE_CUDA(cudaSetDevice(t->device));
+    cudaStream_t st = (cudaStream_t)p2p_session_stream(s);
+    tree_unpermute_kernel<<<grid(t->npart, 256, 8192), 256, 0, st>>>(d_in, t->perm, t->npart, d_out);
+    TREE_CUDA(cudaGetLastError());
+    count_launches(1);
     return P2P_OK;
 }
 

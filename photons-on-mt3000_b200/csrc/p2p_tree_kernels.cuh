@@ -151,15 +151,31 @@ struct TreeSeg {
     int nsmall, nbig;
 };
 
-// One thread per segment: the split value.
-__global__ void tree_seg_mean_kernel(TreeSeg *segs, int nseg, TreeParts P, TreeRec R) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nseg) return;
-    TreeSeg g = segs[s];
-    const double *c = g.axis == 0 ? P.x : (g.axis == 1 ? P.y : P.z);
-    g.mean = tree_mean(c + g.ipart, g.length);
-    segs[s].mean = g.mean;
-    R.split[g.node] = g.mean;
+// One block per segment: the split value. The samples are gathered into
+// shared memory by the whole block, a chunk at a time, and summed in slot
+// order by one thread (the reference's rounding sequence, tree_mean).
+constexpr int kTreeMeanChunk = 4096;
+__global__ void __launch_bounds__(kTreeThreads) tree_seg_mean_kernel(TreeSeg *segs, TreeParts P, TreeRec R) {
+    __shared__ double buf[kTreeMeanChunk];
+    const TreeSeg g = segs[blockIdx.x];
+    const double *c = (g.axis == 0 ? P.x : (g.axis == 1 ? P.y : P.z)) + g.ipart;
+    int mul = 1;
+    if (g.length > 100000) mul = g.length / 100000;
+    const int nsamp = (g.length + mul - 1) / mul;  // slots 0, mul, 2 mul, ... < length
+    double mean = 0.0;
+    for (int s0 = 0; s0 < nsamp; s0 += kTreeMeanChunk) {
+        const int ns = min(kTreeMeanChunk, nsamp - s0);
+        for (int i = threadIdx.x; i < ns; i += blockDim.x) buf[i] = c[(size_t)(s0 + i) * mul];
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int i = 0; i < ns; ++i) mean = __dadd_rn(mean, buf[i]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        mean = __dmul_rn(__ddiv_rn(mean, (double)g.length), (double)mul);
+        segs[blockIdx.x].mean = mean;
+        R.split[g.node] = mean;
+    }
 }
 
 // Tiles of kTreeTile slots: tile t covers slots [tile_off[t], +kTreeTile) of
@@ -569,6 +585,19 @@ __global__ void tree_active_kernel(const int *__restrict__ leaf_ipart, const int
         for (int q = lane; q < np; q += 32) any = any || (tag ? tag[id[ip + q]] == 1 : true);
         any = __any_sync(0xffffffffu, any);
         if (lane == 0) active[l] = any ? 0 : -1;
+    }
+}
+
+// A per-particle SoA result in tree order back to input order:
+// out[d * n + perm[i]] = in[d * n + i].
+__global__ void tree_unpermute_kernel(const double *__restrict__ in, const int *__restrict__ perm, int n,
+                                      double *__restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = perm[i];
+        if ((unsigned)j >= (unsigned)n) continue;
+        out[j] = in[i];
+        out[(size_t)n + j] = in[(size_t)n + i];
+        out[2 * (size_t)n + j] = in[2 * (size_t)n + i];
     }
 }
 

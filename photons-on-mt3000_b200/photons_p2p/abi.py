@@ -153,6 +153,7 @@ SIGNATURES = {
                                      ctypes.POINTER(_vp)]),
     "p2p_dtree_walk_tree": (_i, [_vp, ctypes.POINTER(WalkTree)]),
     "p2p_dtree_download": (_i, [_vp] + [_vp] * 11),
+    "p2p_dtree_unpermute": (_i, [_vp, _vp, _vp, _vp]),
     "p2p_host_alloc": (_i, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "p2p_host_free": (_i, [_vp]),
 }

@@ -33,7 +33,7 @@ CANDIDATES = [
     (v, st, w) for v in (abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SOURCE_LANES_X2_S16)
     for st in (128, 256, 512) for w in (2, 4)
 ] + [(abi.VARIANT_SINK_LANES_X2, st, w) for st in (128, 256, 512) for w in (2, 4)
-] + [(abi.VARIANT_SINK_REGS, st, w) for st in (256, 512) for w in (2, 4)]
+] + [(abi.VARIANT_SINK_REGS, st, w) for st in (256, 384) for w in (2, 4)]
 
 
 def histogram_key(leaf_npart, task_t, form, soft_mode):

@@ -248,6 +248,11 @@ class DeviceTree:
         _check(self.lib, self.lib.p2p_dtree_device_arrays(self.h, *[ctypes.byref(x) for x in p]))
         return tuple(x.value for x in p)
 
+    def unpermute(self, d_in, d_out):
+        """d_out (input order) from d_in (tree order): device pointers of
+        3*npart doubles, queued on the session's stream."""
+        _check(self.lib, self.lib.p2p_dtree_unpermute(self.h, self.session.h, d_in, d_out))
+
     def download(self):
         """Host copies: dict of pos (3, n), perm, leaf_ipart, leaf_npart,
         leaf_active, leaf_center (nleaf, 3), leaf_width, son (nnode, 2),

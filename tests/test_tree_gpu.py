@@ -101,5 +101,11 @@ def test_pass_on_device_tree_equals_host_lists(gpu):
                 got = np.zeros((3, t.npart))
                 s.accumulate(got)
                 assert ntask == tl.ntask and s.pair_count() == ref_pairs
+                # the result in the input order of the positions
+                d_out = torch.empty((3, t.npart), dtype=torch.float64, device=dev)
+                t.unpermute(s.result_device(), d_out.data_ptr())
+                s.lib.p2p_session_synchronize(s.h)
+                back = d_out.cpu().numpy()
+                assert np.array_equal(back[:, tl.perm], got)
         rms, mx = rel_err(got, ref, tl.tag == 1)
         assert mx <= (1e-13 if form == abi.FORM_PLAIN_FP64 else 1e-5), (form, rms, mx)
