@@ -21,6 +21,10 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
            H2D of positions, leaves and lists, the pass, D2H of the forces
   roofline FP32 pipe: pairs/s x flops-per-pair (counted from the kernel
            source, FMA = 2) / the FP32 FFMA peak measured in-process
+  pm       the PM long-range force (deposit, FFT, Green's function, FFT,
+           gradient, interpolation) on the workload's particles and mesh:
+           device ms per phase, the gradient kernel's HBM roofline, and the
+           numpy PM oracle beside the GPU on the 32^3 / mesh 64^3 workload
   serving  48 boxes of the serving ensemble resident in one server:
            saturation throughput, then Poisson arrivals at half of it,
            p50 / p99 request latency (submit to result in host memory)
@@ -130,6 +134,16 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
                 "samples": len(self.rows)}
+
+
+def measured_hbm_peak():
+    """The pool's measured copy bandwidth (GB/s) from MEASURED_PEAKS.json, or
+    the earlier measurement 6650 GB/s when the file is absent."""
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def load_traffic(workload, form_name):
@@ -268,6 +282,60 @@ def device_tree_leg(sess, cfg, allpos, tag, dev, host_perm, host_ip, pairs, step
            "tree_equal_host": equal, "pairs_equal": bool(got_pairs == pairs),
            "pairs_per_s": pairs / float(np.mean(total_s))}
     out["e2e_particles"] = particles_e2e(sess, cfg, allpos, tag, dev, pairs, steps)
+    return out
+
+
+def pm_leg(sess, cfg, raw_pos, dev, hbm_peak, cpu=True, steps=5, warmup=3):
+    """The PM long-range force (p2p_pm_forces) on the workload's local
+    particles and mesh: device times per phase (CUDA events on the session's
+    stream), in the particles' input order and sorted by mesh cell (the order
+    a tree walk leaves them in), the gradient kernel against the HBM roofline
+    (8 bytes read and 24 written per cell), and the numpy oracle beside the
+    GPU on the lattice drop-in workload (32^3 particles, mesh 64^3)."""
+    import torch
+
+    from oracle import pm_oracle as PMO
+    from photons_p2p.p2p import ParticleMesh
+
+    n = raw_pos.shape[1]
+    mass = 1.0 / n
+    cell = np.minimum((raw_pos * (cfg.mesh / cfg.box)).astype(np.int64), cfg.mesh - 1)
+    order = np.argsort((cell[0] * cfg.mesh + cell[1]) * cfg.mesh + cell[2], kind="stable")
+    out = {"mesh": cfg.mesh, "particles": n}
+
+    def timed(pm, pos, nsteps, nwarm):
+        d_pos = torch.from_numpy(np.ascontiguousarray(pos)).to(dev)
+        d_acc = torch.empty_like(d_pos)
+        torch.cuda.synchronize()
+        rows = []
+        for k in range(nwarm + nsteps):
+            pm.forces(d_pos, None, mass, d_acc)
+            t = pm.timings()
+            if k >= nwarm:
+                rows.append(t)
+        return {key: float(np.mean([r[key] for r in rows])) for key in rows[0]}
+
+    with ParticleMesh(sess, cfg.mesh, cfg.box, cfg.split_radius) as pm:
+        out["input_order_ms"] = timed(pm, raw_pos, steps, warmup)
+        out["cell_sorted_ms"] = timed(pm, raw_pos[:, order], steps, warmup)
+    ms = out["cell_sorted_ms"]
+    out["particles_per_s"] = n / (ms["total"] * 1e-3)
+    grad_bytes = 32.0 * cfg.mesh ** 3
+    achieved = grad_bytes / (ms["gradient"] * 1e-3) / 1e9
+    out["gradient_roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                                "frac": achieved / hbm_peak, "bytes_per_cell": 32}
+    if not cpu:
+        return out
+    # the oracle beside the GPU on the lattice drop-in workload
+    c1 = W.c1_config()
+    p1 = W.c1_positions()
+    t0 = time.perf_counter()
+    PMO.pm_forces(p1, None, 1.0 / p1.shape[1], c1.mesh, c1.box, c1.split_radius)
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    with ParticleMesh(sess, c1.mesh, c1.box, c1.split_radius) as pm:
+        gpu1 = timed(pm, p1, steps, warmup)
+    out["lattice_32^3_mesh_64^3"] = {"gpu_ms": gpu1["total"], "cpu_oracle_ms": cpu_ms,
+                                     "cpu_oracle": "numpy, 1 thread (the reference's PM needs MPI and 2DECOMP&FFT)"}
     return out
 
 
@@ -435,6 +503,10 @@ def run_ours(args, rank, world, dist):
         walk = None
         if not args.no_walk:
             walk = walk_leg(sess, cfg, raw_pos, tl, dev, d_pos, d_ip, d_np, P)
+        pm = None
+        if not args.no_pm:
+            pm = pm_leg(sess, cfg, raw_pos, dev, measured_hbm_peak(),
+                        cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     mean_pass = float(np.mean(pass_s))
     mean_kernel_ms = float(np.mean(kern_ms))
@@ -476,6 +548,7 @@ def run_ours(args, rank, world, dist):
         "plain_fp64": plain,
         "split_over_plain": (value / plain["value"]) if plain else None,
         "device_walk": walk,
+        "pm": pm,
         "accuracy": accuracy,
         "e2e": {"value": P_all / e2e_mean, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -796,6 +869,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving summary")
     ap.add_argument("--no-walk", action="store_true", help="skip the device list walk leg")
+    ap.add_argument("--no-pm", action="store_true", help="skip the PM long-range leg")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape, no autotuning")
     ap.add_argument("--boxes", type=int, default=512, help="c4: ensemble size")
     ap.add_argument("--slots", type=int, default=1, help="c4: server launch slots")

@@ -223,6 +223,32 @@ int p2p_dtree_download(const p2p_dtree *t, double *pos, int *perm, int *leaf_ipa
                        int *leaf_active, double *leaf_center, double *leaf_width, int *son, int *node_first,
                        double *node_center, double *node_width);
 
+/* ---- Particle-mesh long-range force (the TreePM complement) ------------
+ * Replaces partmesh_kick's force part (src/partmesh.c:12-1470 with
+ * src/conv.f90:239-330) for one periodic domain: cloud-in-cell deposit of
+ * the particles with tag 1, scaled to density by (N/L)^3, FFT, times the
+ * Green's function pref exp(-k2 (2 pi r_s / L)^2) / k2 / (sinc_x sinc_y
+ * sinc_z)^4 (integer wave numbers, pref = L^2 / (pi N^3), zero mode 0),
+ * inverse FFT without normalisation, the 4-point difference (4/3, 1/6,
+ * step N / (2 L)) per axis, cloud-in-cell interpolation. The reference's MPI
+ * sub-domains and halos become periodic wraps; the FFTs are cuFFT (the
+ * reference calls FFTW through 2DECOMP&FFT). Meshes: N^3 doubles (mass,
+ * potential), 3 N^3 (gradient), N^2 (N/2 + 1) complex, allocated at create.
+ * nmesh even in [4, 1024]; positions in [0, boxsize). */
+typedef struct p2p_pm p2p_pm;
+int p2p_pm_create(p2p_session *s, int nmesh, double boxsize, double split_radius, p2p_pm **out);
+int p2p_pm_destroy(p2p_pm *pm);
+/* Queues the PM force on the session's stream: d_pos 3*npart doubles (SoA,
+ * device), d_tag nullable (all tag 1), equal masses; d_acc (3*npart doubles,
+ * SoA, device) receives the long-range acceleration, 0 for tag != 1. */
+int p2p_pm_forces(p2p_pm *pm, int npart, const double *d_pos, const int *d_tag, double mass, double *d_acc);
+/* Device times in ms of the last p2p_pm_forces (waits for it): deposit,
+ * FFT-Green-FFT, gradient, interpolation, total. */
+int p2p_pm_timings(p2p_pm *pm, float ms[5]);
+/* Host copies of the last deposit (mass per cell, index (x N + y) N + z) and
+ * potential (nullable outputs, N^3 doubles each). */
+int p2p_pm_download(p2p_pm *pm, double *mass_mesh, double *potential);
+
 /* Host copy of the CSR rows of the last submitted chunk or walk (row_off:
  * nleaf+1 entries; row_src (nullable: rows not copied): row_off[nleaf]
  * entries). Call after p2p_pass_end. */

@@ -1,6 +1,7 @@
 """Build recipe for the native libraries of the package.
 
-    libphotons_p2p.so    CUDA P2P pass for sm_100a + its C ABI (csrc/*.cu)
+    libphotons_p2p.so    CUDA P2P pass for sm_100a + its C ABI (csrc/*.cu); the PM
+                         long-range force links cuFFT for its two FFTs
     libphotons_lists.so  host tree build / interaction-list walk (host/*.cpp)
 
 Both land in photons_p2p/ next to the Python bindings, so a snapshot of the
@@ -20,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu", "p2p_pair_sink_lanes.cu", "p2p_pair_source_lanes.cu",
                 "p2p_pair_source_lanes_x2.cu", "p2p_pair_source_lanes_x2_kahan.cu",
                 "p2p_pair_source_lanes_x2_f32.cu", "p2p_pair_plain.cu", "p2p_server.cu", "p2p_pair_sink_lanes_x2.cu",
-                "p2p_pair_sink_regs.cu", "p2p_tree.cu"]
+                "p2p_pair_sink_regs.cu", "p2p_tree.cu", "p2p_pm.cu"]
 CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_pass_kernels.cuh", "p2p_pair_kernels.cuh",
                 "p2p_device_common.cuh", "p2p_launch.h", "p2p_internal.h", "p2p_fit.h",
                 "p2p_pair_x2_impl.h", "p2p_csr.h", "p2p_args.h", "p2p_host_shared.h", "p2p_walk_kernels.cuh",
@@ -68,7 +69,9 @@ def build_cuda(force=False, extra=()):
     objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
     with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
         list(ex.map(lambda so: _run([NVCC] + flags + ["-c", so[0], "-o", so[1]]), zip(srcs, objs)))
-    _run([NVCC] + GENCODE + ["--shared", "-o", target] + objs)
+    cudalib = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
+    _run([NVCC] + GENCODE + ["--shared", "-o", target] + objs +
+         ["-L", cudalib, "-lcufft", "-Xlinker", "-rpath," + cudalib])
     return target
 
 

@@ -154,6 +154,11 @@ SIGNATURES = {
     "p2p_dtree_walk_tree": (_i, [_vp, ctypes.POINTER(WalkTree)]),
     "p2p_dtree_download": (_i, [_vp] + [_vp] * 11),
     "p2p_dtree_unpermute": (_i, [_vp, _vp, _vp, _vp]),
+    "p2p_pm_create": (_i, [_vp, _i, _d, _d, ctypes.POINTER(_vp)]),
+    "p2p_pm_destroy": (_i, [_vp]),
+    "p2p_pm_forces": (_i, [_vp, _i, _vp, _vp, _d, _vp]),
+    "p2p_pm_timings": (_i, [_vp, ctypes.POINTER(ctypes.c_float)]),
+    "p2p_pm_download": (_i, [_vp, _vp, _vp]),
     "p2p_host_alloc": (_i, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "p2p_host_free": (_i, [_vp]),
 }

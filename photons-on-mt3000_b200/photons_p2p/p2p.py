@@ -220,6 +220,62 @@ class DeviceWalkTree:
                                    t[6].data_ptr())
 
 
+class ParticleMesh:
+    """The PM long-range force (p2p_pm_*): PhotoNs' partmesh_kick force part
+    (src/partmesh.c:12-1470, src/conv.f90:239-330) for one periodic domain on
+    the session's device and stream."""
+
+    def __init__(self, session, nmesh, boxsize, split_radius):
+        self.lib = session.lib
+        self.session = session
+        self.nmesh = int(nmesh)
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.p2p_pm_create(session.h, self.nmesh, float(boxsize), float(split_radius),
+                                                ctypes.byref(h)))
+        self.h = h
+
+    def forces(self, pos_dev, tag_dev, mass, acc_dev):
+        """Queues the long-range accelerations of the particles with tag 1 into
+        acc_dev: torch float64 (3, n) tensors on the device (SoA rows), tag_dev
+        int32 (n,) or None (all tag 1)."""
+        n = int(pos_dev.shape[-1])
+        _check(self.lib, self.lib.p2p_pm_forces(self.h, n, pos_dev.data_ptr(),
+                                                tag_dev.data_ptr() if tag_dev is not None else None,
+                                                float(mass), acc_dev.data_ptr()))
+
+    def timings(self):
+        """Device ms of the last forces(): deposit, fft_green_fft, gradient,
+        interp, total."""
+        ms = (ctypes.c_float * 5)()
+        _check(self.lib, self.lib.p2p_pm_timings(self.h, ms))
+        return dict(zip(["deposit", "fft_green_fft", "gradient", "interp", "total"], list(ms)))
+
+    def download(self):
+        """Host copies (mass per cell, potential), each (n, n, n) indexed [x, y, z]."""
+        n = self.nmesh
+        mass, phi = np.empty((n, n, n)), np.empty((n, n, n))
+        _check(self.lib, self.lib.p2p_pm_download(self.h, mass.ctypes.data_as(ctypes.c_void_p),
+                                                  phi.ctypes.data_as(ctypes.c_void_p)))
+        return mass, phi
+
+    def close(self):
+        if self.h:
+            self.lib.p2p_pm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DeviceTree:
     """The kd-tree built on the GPU (p2p_dtree_build): the tree PhotoNs builds
     on the host before its walk (src/fmm.c:69-327), equal node for node.
