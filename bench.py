@@ -1,7 +1,7 @@
 """Benchmark of the B200 P2P short-range force pass.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload c2|c1|c2_128|c4] [--form split|plain]
+                [--workload c2|c1|c2_128|c4|pm] [--form split|plain]
 
 A step is one force pass over the workload's interaction lists. The default
 workload is the 256^3 clustered configuration (60% uniform, 40% in 2,000 NFW
@@ -23,7 +23,7 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
            source, FMA = 2) / the FP32 FFMA peak measured in-process
   pm       the PM long-range force (deposit, FFT, Green's function, FFT,
            gradient, interpolation) on the workload's particles and mesh:
-           device ms per phase, the gradient kernel's HBM roofline, and the
+           device ms per phase, the deposit and force kernels' HBM roofline, the
            numpy PM oracle beside the GPU on the 32^3 / mesh 64^3 workload
   serving  48 boxes of the serving ensemble resident in one server:
            saturation throughput, then Poisson arrivals at half of it,
@@ -31,6 +31,7 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
 
 --workload c4 runs the serving configuration alone: 512 boxes, Poisson
 arrivals at 0.25, 0.5, 1, 2 and 4 times the measured saturation rate.
+--workload pm runs the PM leg alone (256^3 clustered particles, mesh 256^3).
 
 With --gpus N > 1 (torchrun, one rank per GPU) every rank runs its own
 independent box (replicas, no collective on the data path); the timed
@@ -289,8 +290,8 @@ def pm_leg(sess, cfg, raw_pos, dev, hbm_peak, cpu=True, steps=5, warmup=3):
     """The PM long-range force (p2p_pm_forces) on the workload's local
     particles and mesh: device times per phase (CUDA events on the session's
     stream), in the particles' input order and sorted by mesh cell (the order
-    a tree walk leaves them in), the gradient kernel against the HBM roofline
-    (8 bytes read and 24 written per cell), and the numpy oracle beside the
+    a tree walk leaves them in), the deposit and force kernels against the
+    HBM roofline of their algorithmic bytes, and the numpy oracle beside the
     GPU on the lattice drop-in workload (32^3 particles, mesh 64^3)."""
     import torch
 
@@ -320,10 +321,17 @@ def pm_leg(sess, cfg, raw_pos, dev, hbm_peak, cpu=True, steps=5, warmup=3):
         out["cell_sorted_ms"] = timed(pm, raw_pos[:, order], steps, warmup)
     ms = out["cell_sorted_ms"]
     out["particles_per_s"] = n / (ms["total"] * 1e-3)
-    grad_bytes = 32.0 * cfg.mesh ** 3
-    achieved = grad_bytes / (ms["gradient"] * 1e-3) / 1e9
-    out["gradient_roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                                "frac": achieved / hbm_peak, "bytes_per_cell": 32}
+    # algorithmic HBM bytes: deposit reads positions (24 B a particle) and
+    # writes the mass mesh (8 B a cell, cleared and summed); the gradient
+    # reads the potential (8 B a cell) and writes the interleaved gradient
+    # (32 B); interpolation reads positions and the gradient mesh once and
+    # writes accelerations (24 B a particle)
+    cells = float(cfg.mesh) ** 3
+    for name, nbytes in (("deposit", 24.0 * n + 16.0 * cells), ("gradient", 40.0 * cells),
+                         ("interp", 48.0 * n + 32.0 * cells)):
+        achieved = nbytes / (ms[name] * 1e-3) / 1e9
+        out[f"{name}_roofline"] = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                                   "frac": achieved / hbm_peak, "bytes": nbytes}
     if not cpu:
         return out
     # the oracle beside the GPU on the lattice drop-in workload
@@ -922,6 +930,26 @@ def main():
     if args.workload == "c3":
         if rank == 0:
             print(json.dumps(run_batching(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "pm":
+        # the PM long-range force alone on the 256^3 clustered particles and
+        # mesh (the default workload's PM leg, without the P2P pass)
+        if rank == 0:
+            import torch
+
+            from photons_p2p.p2p import Session
+
+            local = int(os.environ.get("LOCAL_RANK", "0"))
+            torch.cuda.set_device(local)
+            with Session(local) as sess:
+                pm = pm_leg(sess, W.c2_config(), W.c2_positions(), torch.device("cuda", local),
+                            measured_hbm_peak(), cpu=not args.no_cpu_baseline, steps=args.steps,
+                            warmup=args.warmup)
+            print(json.dumps({"workload": "pm_clustered_256^3_mesh_256^3", "pm": pm}), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

@@ -232,8 +232,9 @@ int p2p_dtree_download(const p2p_dtree *t, double *pos, int *perm, int *leaf_ipa
  * inverse FFT without normalisation, the 4-point difference (4/3, 1/6,
  * step N / (2 L)) per axis, cloud-in-cell interpolation. The reference's MPI
  * sub-domains and halos become periodic wraps; the FFTs are cuFFT (the
- * reference calls FFTW through 2DECOMP&FFT). Meshes: N^3 doubles (mass,
- * potential), 3 N^3 (gradient), N^2 (N/2 + 1) complex, allocated at create.
+ * reference calls FFTW through 2DECOMP&FFT). Device memory: N^3 doubles
+ * (mass), N^3 (potential), 4 N^3 (interleaved gradient), N^2 (N/2 + 1)
+ * complex, allocated at create.
  * nmesh even in [4, 1024]; positions in [0, boxsize). */
 typedef struct p2p_pm p2p_pm;
 int p2p_pm_create(p2p_session *s, int nmesh, double boxsize, double split_radius, p2p_pm **out);

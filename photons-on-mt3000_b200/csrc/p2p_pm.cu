@@ -12,9 +12,11 @@
 //             mode 0 (src/conv.f90:239-316), complex-to-real FFT without
 //             normalisation (pm_green_kernel is this file's own)
 //   gradient  the reference's 4-point difference f1 h (M[+1] - M[-1]) -
-//             f2 h (M[+2] - M[-2]), f1 = 4/3, f2 = 1/6, h = N / (2 L), per axis,
-//             into three meshes (src/partmesh.c:1209-1262)
-//   interp    cloud-in-cell weights of the deposit on the 8 cells' gradients
+//             f2 h (M[+2] - M[-2]), f1 = 4/3, f2 = 1/6, h = N / (2 L), per axis
+//             (src/partmesh.c:1116-1262), for every cell into one interleaved
+//             mesh (gx, gy, gz, 0): 32 bytes, one sector, per cell
+//   interp    per particle, the 8 cloud-in-cell cells' gradients weighted as
+//             in the deposit and summed in the reference's cell order
 //             (src/partmesh.c:1415-1450)
 // The reference splits the mesh over MPI sub-domains with halos; on one
 // periodic domain every halo read is a periodic wrap. The FFTs are cuFFT
@@ -23,8 +25,10 @@
 #include <cuda_runtime.h>
 #include <cufft.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "photons_p2p.h"
 #include "p2p_host_shared.h"
@@ -40,7 +44,8 @@ struct p2p_pm {
     double *density = nullptr;      // N^3, mass per cell
     cufftDoubleComplex *spec = nullptr;  // N * N * (N/2 + 1)
     double *potential = nullptr;    // N^3
-    double *grad = nullptr;         // 3 * N^3
+    double4 *grad = nullptr;        // N^3 cells of (gx, gy, gz, 0)
+    double *sinc = nullptr;         // N: sin(pi l / N) / (pi l / N), l the wrapped index
     cufftHandle fwd = 0, inv = 0;
     bool fwd_ok = false, inv_ok = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -72,86 +77,125 @@ __device__ __forceinline__ void cic_axis(double x, double norm, double delta, in
     w = d;
 }
 
-__global__ void pm_deposit_kernel(const double *__restrict__ pos, const int *__restrict__ tag, int npart,
-                                  double mass, int n, double norm, double delta, double *__restrict__ mesh) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npart; p += gridDim.x * blockDim.x) {
-        if (tag && tag[p] != 1) continue;
-        int c[3], nb[3];
-        double w[3];
-        for (int a = 0; a < 3; ++a) cic_axis(pos[(size_t)a * npart + p], norm, delta, n, c[a], nb[a], w[a]);
+constexpr unsigned kFull = 0xffffffffu;
+
+// Cloud-in-cell deposit, one particle per lane. Whole warps stay converged
+// (the loop bound is per warp) so that each of the 8 corners can first be
+// summed over lanes that hold the same cell in a run (particles in the same
+// cell, next to each other in the input, as in tree or cell order): a
+// segmented scan over the lanes, as many steps as the longest run needs,
+// then one FP64 atomic per run. A warp whose lanes all differ skips the scan.
+__global__ void __launch_bounds__(256) pm_deposit_kernel(const double *__restrict__ pos, const int *__restrict__ tag,
+                                                         int npart, double mass, int n, double norm, double delta,
+                                                         double *__restrict__ mesh) {
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + threadIdx.x - lane; base < npart; base += stride) {
+        const int p = base + lane;
+        const bool on = p < npart && (!tag || tag[p] == 1);
+        int c[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
+        double w[3] = {0.0, 0.0, 0.0};
+        if (on)
+            for (int a = 0; a < 3; ++a) cic_axis(pos[(size_t)a * npart + p], norm, delta, n, c[a], nb[a], w[a]);
+#pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int ix = (q & 1) ? nb[0] : c[0], iy = (q & 2) ? nb[1] : c[1], iz = (q & 4) ? nb[2] : c[2];
             const double wx = (q & 1) ? w[0] : 1.0 - w[0], wy = (q & 2) ? w[1] : 1.0 - w[1],
                          wz = (q & 4) ? w[2] : 1.0 - w[2];
-            atomicAdd(&mesh[((size_t)ix * n + iy) * n + iz], __dmul_rn(__dmul_rn(__dmul_rn(mass, wx), wy), wz));
+            const int key = on ? (ix * n + iy) * n + iz : -1;
+            double v = on ? __dmul_rn(__dmul_rn(__dmul_rn(mass, wx), wy), wz) : 0.0;
+            const int prev = __shfl_up_sync(kFull, key, 1), next = __shfl_down_sync(kFull, key, 1);
+            const bool head = lane == 0 || prev != key, tail = lane == 31 || next != key;
+            const unsigned heads = __ballot_sync(kFull, head);
+            if (heads != kFull) {
+                // sum each run of equal keys into its last lane: a scan over
+                // the lanes that adds lane - d only while it is in the run
+                const unsigned upto = heads & (0xffffffffu >> (31 - lane));
+                const int first = 31 - __clz(upto);
+                const int depth = __reduce_max_sync(kFull, (unsigned)(lane - first));
+                for (int d = 1; d <= depth; d <<= 1) {
+                    const double vu = __shfl_up_sync(kFull, v, d);
+                    if (lane - d >= first) v = __dadd_rn(vu, v);
+                }
+            }
+            if (tail && key >= 0) atomicAdd(&mesh[key], v);
         }
     }
 }
 
-__device__ __forceinline__ double sinc_mode(int l, int n) {
-    if (l == 0) return 1.0;
-    const double a = M_PI * (double)l / (double)n;
-    return sin(a) / a;
-}
-
-// The Green's function on the half spectrum (z halved): l, m from the x, y
-// indices (wrapped above N/2), n from z.
-__global__ void pm_green_kernel(cufftDoubleComplex *__restrict__ spec, int n, double s2, double pref,
-                                double renormal) {
+// The Green's function on the half spectrum (z halved): block row y is the
+// x index i, the flattened (j, kz) runs over threads; l, m are i, j wrapped
+// above N/2, n = kz.
+__global__ void pm_green_kernel(cufftDoubleComplex *__restrict__ spec, const double *__restrict__ sinc, int n,
+                                double s2, double pref, double renormal) {
     const int nz = n / 2 + 1;
-    const size_t total = (size_t)n * n * nz;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int kz = (int)(q % nz);
-        const int j = (int)((q / nz) % n);
-        const int i = (int)(q / ((size_t)nz * n));
-        const int l = i > n / 2 ? i - n : i, m = j > n / 2 ? j - n : j, k = kz;
-        double g = 0.0;
-        if (l != 0 || m != 0 || k != 0) {
-            const double k2 = (double)(l * l + m * m + k * k);
-            const double ff = 1.0 / (sinc_mode(l, n) * sinc_mode(m, n) * sinc_mode(k, n));
-            g = pref * (exp(-k2 * s2) / k2 * (ff * ff * ff * ff)) * renormal;
-        }
-        spec[q].x *= g;
-        spec[q].y *= g;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * nz) return;
+    const int i = blockIdx.y, j = t / nz, kz = t - j * nz;
+    const int l = i > n / 2 ? i - n : i, m = j > n / 2 ? j - n : j;
+    const size_t q = (size_t)i * n * nz + t;
+    double g = 0.0;
+    if (l != 0 || m != 0 || kz != 0) {
+        const double k2 = (double)(l * l + m * m + kz * kz);
+        const double ff = 1.0 / (sinc[i] * sinc[j] * sinc[kz]);
+        g = pref * (exp(-k2 * s2) / k2 * (ff * ff * ff * ff)) * renormal;
     }
+    spec[q].x *= g;
+    spec[q].y *= g;
 }
 
-__global__ void pm_gradient_kernel(const double *__restrict__ phi, int n, double h, double *__restrict__ grad) {
-    const size_t total = (size_t)n * n * n;
-    const double f1 = 4.0 / 3.0, f2 = 1.0 / 6.0;
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (size_t)gridDim.x * blockDim.x) {
-        const int k = (int)(q % n), j = (int)((q / n) % n), i = (int)(q / ((size_t)n * n));
-        const int c[3] = {i, j, k};
-        for (int a = 0; a < 3; ++a) {
-            int cm1[3] = {i, j, k}, cp1[3] = {i, j, k}, cm2[3] = {i, j, k}, cp2[3] = {i, j, k};
-            cm1[a] = wrap(c[a] - 1, n);
-            cp1[a] = wrap(c[a] + 1, n);
-            cm2[a] = wrap(c[a] - 2, n);
-            cp2[a] = wrap(c[a] + 2, n);
-            auto at = [&](const int *v) { return phi[((size_t)v[0] * n + v[1]) * n + v[2]]; };
-            const double d1 = at(cp1) - at(cm1), d2 = at(cp2) - at(cm2);
-            grad[(size_t)a * total + q] = __dsub_rn(__dmul_rn(__dmul_rn(f1, h), d1), __dmul_rn(__dmul_rn(f2, h), d2));
-        }
-    }
+__device__ __forceinline__ int wrap_near(int i, int n) {
+    return i < 0 ? i + n : (i >= n ? i - n : i);
 }
 
-__global__ void pm_interp_kernel(const double *__restrict__ pos, const int *__restrict__ tag, int npart, int n,
-                                 double norm, double delta, const double *__restrict__ grad,
-                                 double *__restrict__ acc) {
-    const size_t total = (size_t)n * n * n;
+// The 4-point difference along one axis: row = the cell's offset without
+// this axis, v = its coordinate on the axis, s = the axis's stride.
+__device__ __forceinline__ double diff4(const double *__restrict__ phi, size_t row, int v, int n, size_t s,
+                                       double f1h, double f2h) {
+    const double m1 = __ldg(phi + row + (size_t)wrap_near(v - 1, n) * s);
+    const double p1 = __ldg(phi + row + (size_t)wrap_near(v + 1, n) * s);
+    const double m2 = __ldg(phi + row + (size_t)wrap_near(v - 2, n) * s);
+    const double p2 = __ldg(phi + row + (size_t)wrap_near(v + 2, n) * s);
+    return __dsub_rn(__dmul_rn(f1h, __dsub_rn(p1, m1)), __dmul_rn(f2h, __dsub_rn(p2, m2)));
+}
+
+// One cell per thread: block row y is the x index i, the flattened (j, k)
+// runs over threads, so a warp reads and writes consecutive z.
+__global__ void __launch_bounds__(256) pm_gradient_kernel(const double *__restrict__ phi, int n, double f1h,
+                                                          double f2h, double4 *__restrict__ grad) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * n) return;
+    const int i = blockIdx.y, j = t / n, k = t - j * n;
+    const size_t sx = (size_t)n * n, sy = n;
+    double2 *out = reinterpret_cast<double2 *>(grad + (size_t)i * sx + t);
+    const double gx = diff4(phi, (size_t)j * sy + k, i, n, sx, f1h, f2h);
+    const double gy = diff4(phi, (size_t)i * sx + k, j, n, sy, f1h, f2h);
+    const double gz = diff4(phi, (size_t)i * sx + (size_t)j * sy, k, n, 1, f1h, f2h);
+    out[0] = make_double2(gx, gy);
+    out[1] = make_double2(gz, 0.0);
+}
+
+__global__ void __launch_bounds__(256) pm_interp_kernel(const double *__restrict__ pos, const int *__restrict__ tag,
+                                                        int npart, int n, double norm, double delta,
+                                                        const double4 *__restrict__ grad,
+                                                        double *__restrict__ acc) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npart; p += gridDim.x * blockDim.x) {
         double out[3] = {0.0, 0.0, 0.0};
         if (!tag || tag[p] == 1) {
             int c[3], nb[3];
             double w[3];
             for (int a = 0; a < 3; ++a) cic_axis(pos[(size_t)a * npart + p], norm, delta, n, c[a], nb[a], w[a]);
+#pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const int ix = (q & 1) ? nb[0] : c[0], iy = (q & 2) ? nb[1] : c[1], iz = (q & 4) ? nb[2] : c[2];
                 const double wx = (q & 1) ? w[0] : 1.0 - w[0], wy = (q & 2) ? w[1] : 1.0 - w[1],
                              wz = (q & 4) ? w[2] : 1.0 - w[2];
                 const double wt = __dmul_rn(__dmul_rn(wx, wy), wz);
-                const size_t cell = ((size_t)ix * n + iy) * n + iz;
-                for (int a = 0; a < 3; ++a) out[a] = __dadd_rn(out[a], __dmul_rn(wt, grad[(size_t)a * total + cell]));
+                const double2 *g = reinterpret_cast<const double2 *>(grad + ((size_t)ix * n + iy) * n + iz);
+                const double2 gxy = __ldg(g), gz = __ldg(g + 1);
+                out[0] = __dadd_rn(out[0], __dmul_rn(wt, gxy.x));
+                out[1] = __dadd_rn(out[1], __dmul_rn(wt, gxy.y));
+                out[2] = __dadd_rn(out[2], __dmul_rn(wt, gz.x));
             }
         }
         acc[p] = out[0];
@@ -163,7 +207,7 @@ __global__ void pm_interp_kernel(const double *__restrict__ pos, const int *__re
 void destroy(p2p_pm *pm) {
     if (pm->fwd_ok) cufftDestroy(pm->fwd);
     if (pm->inv_ok) cufftDestroy(pm->inv);
-    void *ptrs[] = {pm->density, pm->spec, pm->potential, pm->grad};
+    void *ptrs[] = {pm->density, pm->spec, pm->potential, pm->grad, pm->sinc};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : pm->ev)
@@ -204,11 +248,21 @@ P2P_API int p2p_pm_create(p2p_session *s, int nmesh, double boxsize, double spli
     bool ok = cudaMalloc(&pm->density, sizeof(double) * n3) == cudaSuccess &&
               cudaMalloc(&pm->spec, sizeof(cufftDoubleComplex) * nc) == cudaSuccess &&
               cudaMalloc(&pm->potential, sizeof(double) * n3) == cudaSuccess &&
-              cudaMalloc(&pm->grad, sizeof(double) * 3 * n3) == cudaSuccess;
+              cudaMalloc(&pm->grad, sizeof(double4) * n3) == cudaSuccess &&
+              cudaMalloc(&pm->sinc, sizeof(double) * nmesh) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         destroy(pm);
         return report_error(P2P_ERR_NOMEM, "PM mesh allocation failed");
+    }
+    {
+        std::vector<double> sinc(nmesh);
+        for (int i = 0; i < nmesh; ++i) {
+            const int l = i > nmesh / 2 ? i - nmesh : i;
+            const double a = M_PI * (double)l / (double)nmesh;
+            sinc[i] = l == 0 ? 1.0 : std::sin(a) / a;
+        }
+        ok = cudaMemcpy(pm->sinc, sinc.data(), sizeof(double) * nmesh, cudaMemcpyHostToDevice) == cudaSuccess;
     }
     for (cudaEvent_t &ev : pm->ev)
         if (cudaEventCreate(&ev) != cudaSuccess) ok = false;
@@ -239,7 +293,7 @@ P2P_API int p2p_pm_forces(p2p_pm *pm, int npart, const double *d_pos, const int 
     cudaError_t e = cudaSetDevice(pm->device);
     if (e != cudaSuccess) return fail_cuda(e, "cudaSetDevice");
     const int n = pm->n;
-    const size_t n3 = (size_t)n * n * n, nc = (size_t)n * n * (n / 2 + 1);
+    const size_t n3 = (size_t)n * n * n;
     const double norm = (double)n / pm->box, delta = 1.0 / norm;
     cudaStream_t st = pm->stream;
     const int threads = 256;
@@ -253,14 +307,20 @@ P2P_API int p2p_pm_forces(p2p_pm *pm, int npart, const double *d_pos, const int 
     const double s2 = (2.0 * M_PI * pm->split_radius / pm->box) * (2.0 * M_PI * pm->split_radius / pm->box);
     const double pref = pm->box * pm->box / (M_PI * (double)n * (double)n * (double)n);
     const double renormal = norm * norm * norm;
-    pm_green_kernel<<<grid(nc, threads), threads, 0, st>>>(pm->spec, n, s2, pref, renormal);
+    const int nz = n / 2 + 1;
+    pm_green_kernel<<<dim3((n * nz + threads - 1) / threads, n), threads, 0, st>>>(pm->spec, pm->sinc, n, s2, pref,
+                                                                                   renormal);
     if (cufftExecZ2D(pm->inv, pm->spec, pm->potential) != CUFFT_SUCCESS) return report_error(P2P_ERR_CUDA, "PM inverse FFT failed");
     e = cudaEventRecord(pm->ev[2], st);
     if (e != cudaSuccess) return fail_cuda(e, "PM convolution");
-    pm_gradient_kernel<<<grid(n3, threads), threads, 0, st>>>(pm->potential, n, 0.5 * n / pm->box, pm->grad);
+    const double h = 0.5 * n / pm->box;
+    pm_gradient_kernel<<<dim3((n * n + threads - 1) / threads, n), threads, 0, st>>>(
+        pm->potential, n, (4.0 / 3.0) * h, (1.0 / 6.0) * h, pm->grad);
     e = cudaEventRecord(pm->ev[3], st);
     if (e != cudaSuccess) return fail_cuda(e, "PM gradient");
-    if (npart) pm_interp_kernel<<<grid(npart, threads), threads, 0, st>>>(d_pos, d_tag, npart, n, norm, delta, pm->grad, d_acc);
+    if (npart)
+        pm_interp_kernel<<<grid(npart, threads), threads, 0, st>>>(d_pos, d_tag, npart, n, norm, delta, pm->grad,
+                                                                   d_acc);
     e = cudaEventRecord(pm->ev[4], st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return fail_cuda(e, "PM interpolation");
