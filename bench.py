@@ -27,7 +27,9 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
            numpy PM oracle beside the GPU on the 32^3 / mesh 64^3 workload
   serving  48 boxes of the serving ensemble resident in one server:
            saturation throughput, then Poisson arrivals at half of it,
-           p50 / p99 request latency (submit to result in host memory)
+           p50 / p99 request latency (submit to result in host memory),
+           with the batching window on (launches wait up to 3 mean service
+           times for other requests to share them) and, beside it, off
 
 --workload c4 runs the serving configuration alone: 512 boxes, Poisson
 arrivals at 0.25, 0.5, 1, 2 and 4 times the measured saturation rate.
@@ -590,26 +592,41 @@ def serving_ensemble(srv, nbox, log=None):
     return npart, pairs
 
 
-def serving_measure(srv, rates_frac, requests, seed=10):
+def serving_measure(srv, rates_frac, requests, seed=10, window_service_times=0.0):
     """Saturation throughput (a burst of 2 requests per box), then Poisson
-    arrivals at the given fractions of it."""
+    arrivals at the given fractions of it. window_service_times > 0 sets the
+    server's batching window to that many mean service times (1 / saturation
+    request rate) after the saturation run, with a pack launching without
+    waiting once it holds 3 mean requests' pair interactions."""
     from photons_p2p import serve
 
     nbox = len(srv.boxes)
+    srv.set_batching(0.0)
     sat = serve.run_poisson(srv, 1e9, 2 * nbox, seed=seed, reserve=2)
+    window = None
+    if window_service_times > 0:
+        mean_s = 1.0 / sat["requests_per_s"]
+        mean_pairs = sat["pairs_per_s"] / sat["requests_per_s"]
+        window = {"batch_window_ms": 1e3 * window_service_times * mean_s, "min_pack_pairs": 3.0 * mean_pairs,
+                  "service_times": window_service_times}
+        srv.set_batching(window["batch_window_ms"], window["min_pack_pairs"])
     rows = []
     for i, f in enumerate(rates_frac):
         rate = f * sat["requests_per_s"]
         n = requests(rate) if callable(requests) else requests
         r = serve.run_poisson(srv, rate, int(n), seed=seed + 1 + i)
         r["rate_frac"] = f
+        r["window"] = window
         rows.append(r)
+    srv.set_batching(0.0)
     return sat, rows
 
 
-def run_serving_leg(local, nbox=48):
+def run_serving_leg(local, nbox=48, window_service_times=3.0):
     """The serving summary of the default run: nbox ensemble boxes, one full
-    grid slot, Poisson arrivals at half the measured saturation rate."""
+    grid slot, Poisson arrivals at half the measured saturation rate, with
+    and without the batching window (window_service_times mean service
+    times; launches wait for company up to that long)."""
     from photons_p2p import serve
 
     t0 = time.time()
@@ -618,14 +635,21 @@ def run_serving_leg(local, nbox=48):
         npart, pairs = serving_ensemble(srv, nbox)
         prep = time.time() - t0
         sat, rows = serving_measure(srv, [0.5], 4 * nbox)
-    r = rows[0]
-    return {"boxes": nbox, "particles": int(npart), "slots": 1, "max_pack": 32,
-            "saturation_pairs_per_s": sat["pairs_per_s"],
-            "saturation_requests_per_s": sat["requests_per_s"],
-            "rate_hz": r["rate_hz"], "rate_frac_of_saturation": 0.5, "requests": r["requests"],
-            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "requests_per_s": r["requests_per_s"],
-            "pairs_per_s": r["pairs_per_s"], "boxes_per_launch": r["boxes_per_launch"],
-            "host_prep_s": round(prep, 1)}
+        _, wrows = serving_measure(srv, [0.5], 4 * nbox, seed=20, window_service_times=window_service_times)
+    keys = ("rate_hz", "requests", "p50_ms", "p99_ms", "requests_per_s", "pairs_per_s", "boxes_per_launch")
+    r, w = rows[0], wrows[0]
+    out = {"boxes": nbox, "particles": int(npart), "slots": 1, "max_pack": 32,
+           "saturation_pairs_per_s": sat["pairs_per_s"],
+           "saturation_requests_per_s": sat["requests_per_s"], "rate_frac_of_saturation": 0.5,
+           "host_prep_s": round(prep, 1)}
+    # headline: the batching window on (packs under load); beside it the
+    # same arrivals' rate with the window off (lowest latency at low load)
+    out.update({k: w[k] for k in keys})
+    out["p99_over_p50"] = w["p99_ms"] / w["p50_ms"]
+    out["batch_window"] = w["window"]
+    out["no_window"] = {k: r[k] for k in keys}
+    out["no_window"]["p99_over_p50"] = r["p99_ms"] / r["p50_ms"]
+    return out
 
 
 def run_serving_sweep(args, local):
@@ -645,7 +669,8 @@ def run_serving_sweep(args, local):
         sampler = ClockSampler(local)
         with sampler:
             sat, rows = serving_measure(srv, [0.25, 0.5, 1.0, 2.0, 4.0],
-                                        lambda rate: min(3000, max(200, rate * 6.0)))
+                                        lambda rate: min(3000, max(200, rate * 6.0)),
+                                        window_service_times=args.window)
         st1 = srv.stats()
     for r in rows:
         log(f"[serving] {r['rate_frac']:.2f}x sat ({r['rate_hz']:.0f}/s): p50 {r['p50_ms']:.2f} ms "
@@ -661,6 +686,7 @@ def run_serving_sweep(args, local):
         "config": {"workload": f"c4_serving_{args.boxes}_boxes", "boxes": args.boxes,
                    "particles_with_ghosts": int(npart), "pairs_per_round": int(pairs),
                    "slots": args.slots, "max_pack": 32, "hbm_budget_gb": args.hbm_gb,
+                   "batch_window": rows[0]["window"],
                    "resident_gb": st1["resident_bytes"] / 1e9, "host_prep_s": round(prep, 1),
                    "l2": "inputs > L2 (boxes resident, 126 MB L2)"},
         "serving": {"saturation_pairs_per_s": sat["pairs_per_s"],
@@ -881,6 +907,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default launch shape, no autotuning")
     ap.add_argument("--boxes", type=int, default=512, help="c4: ensemble size")
     ap.add_argument("--slots", type=int, default=1, help="c4: server launch slots")
+    ap.add_argument("--window", type=float, default=0.0,
+                    help="c4: batching window in mean service times (0: off)")
     ap.add_argument("--hbm-gb", type=float, default=100.0, help="c4: server arena size")
     ap.add_argument("--side", type=int, default=512, help="c3: particles per side")
     ap.add_argument("--leaf-caps", default="16,32,64", help="c3: leaf caps to sweep")

@@ -343,6 +343,12 @@ typedef struct {
     size_t hbm_bytes;          /* device memory for resident boxes; 0: half the free memory */
     double rows_per_particle;  /* arena split hint: list entries per particle; 0: 24 */
     double particles_per_leaf; /* arena split hint; 0: 16 */
+    double batch_window_ms;    /* 0 (default): a free slot launches whatever is pending.
+                                  > 0: pending requests wait up to this long (from the
+                                  oldest one's submit) for others to share their launch,
+                                  unless the pack already holds max_pack boxes or
+                                  min_pack_pairs pair interactions; at most 1e4 */
+    double min_pack_pairs;     /* work at which a pack launches without waiting; 0: none */
 } p2p_server_config;
 
 typedef struct {
@@ -396,6 +402,10 @@ int p2p_server_wait(p2p_server *srv, int64_t ticket, double *latency_s);
 int p2p_server_query(p2p_server *srv, int64_t ticket, int *done, double *latency_s);
 /* Blocks until every submitted request has finished. */
 int p2p_server_drain(p2p_server *srv);
+/* Changes the batching window of a running server (the config fields
+ * batch_window_ms and min_pack_pairs); applies from the next scheduling
+ * round. */
+int p2p_server_set_batching(p2p_server *srv, double batch_window_ms, double min_pack_pairs);
 int p2p_server_get_stats(p2p_server *srv, p2p_server_stats *stats);
 /* Page-locked, device-mapped host memory for server results. */
 int p2p_host_alloc(size_t bytes, void **ptr);

@@ -231,6 +231,7 @@ struct Job {
     int box;
     double *out;   // page-locked host buffer
     bool preload;  // make the box resident and pinned; no pass
+    std::chrono::steady_clock::time_point t_submit;
 };
 
 // A launch slot: its compute stream and the copy stream that drains its
@@ -297,6 +298,11 @@ struct p2p_server {
     std::condition_variable cv_work, cv_done;
     uint64_t epoch = 0;            // bumped by completions
     bool stop = false;
+    // batching window: the dispatcher sleeps at most until here; flush: the
+    // server is stopping, launch without waiting (both dispatcher-owned)
+    std::chrono::steady_clock::time_point hold_until = std::chrono::steady_clock::time_point::max();
+    bool flush = false;
+    double set_window_ms = -1.0, set_min_pairs = 0.0;  // p2p_server_set_batching (mu)
     int error = P2P_OK;
     std::string error_msg;
     int64_t submitted = 0, finished = 0;
@@ -699,11 +705,43 @@ int handle_preloads(p2p_server *S) {
     return P2P_OK;
 }
 
+// Batching window (cfg.batch_window_ms > 0): a pack launches at once when it
+// would hold max_pack boxes or cfg.min_pack_pairs pair interactions, or when
+// its oldest request has waited the window; until then the requests wait for
+// others to share the launch, and hold_until tells the dispatcher when to
+// look again. A box not yet built has no pair count and launches at once.
+bool hold_for_window(p2p_server *S) {
+    if (S->cfg.batch_window_ms <= 0.0 || S->flush) return false;
+    std::vector<char> seen(S->nbox_seen, 0);
+    int count = 0;
+    double work = 0.0;
+    Clock::time_point oldest = Clock::time_point::max();
+    for (const Job &j : S->pending) {
+        if (j.preload || S->boxes[j.box].busy || seen[j.box]) continue;
+        seen[j.box] = 1;
+        const Box &b = S->boxes[j.box];
+        if (b.pairs <= 0) return false;
+        work += (double)b.pairs;
+        oldest = std::min(oldest, j.t_submit);
+        if (++count >= S->cfg.max_pack) return false;
+    }
+    if (count == 0) return false;
+    if (S->cfg.min_pack_pairs > 0.0 && work >= S->cfg.min_pack_pairs) return false;
+    const auto until = oldest + std::chrono::duration_cast<Clock::duration>(
+                                    std::chrono::duration<double, std::milli>(S->cfg.batch_window_ms));
+    if (Clock::now() >= until) return false;
+    S->hold_until = std::min(S->hold_until, until);
+    return true;
+}
+
 // One scheduling round: admit and pack pending requests into free slots.
 int schedule(p2p_server *S) {
     P2P_TRY(handle_preloads(S));
+    S->hold_until = Clock::time_point::max();
+    bool held = false;
     for (Slot &sl : S->slots) {
         if (sl.busy) continue;
+        if ((held = hold_for_window(S))) break;
         std::vector<Job> pack;
         std::vector<char> taken(S->nbox_seen, 0);
         bool blocked = false;  // the oldest non-resident box did not fit: admit no later one
@@ -733,9 +771,9 @@ int schedule(p2p_server *S) {
         if (pack.empty()) break;
         P2P_TRY(launch_pack(S, sl, pack));
     }
-    // Nothing in flight and nothing launched: the oldest request's box cannot
-    // be admitted even with every evictable box gone.
-    if (!any_slot_busy(S)) {
+    // Nothing in flight and nothing launched or held: the oldest request's box
+    // cannot be admitted even with every evictable box gone.
+    if (!held && !any_slot_busy(S)) {
         for (auto it = S->pending.begin(); it != S->pending.end(); ++it) {
             if (it->preload) continue;
             S->boxes[it->box].pending--;
@@ -757,7 +795,11 @@ void dispatcher(p2p_server *S) {
         bool stopping;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stop || !S->incoming.empty() || S->epoch != seen; });
+            auto ready = [&] { return S->stop || !S->incoming.empty() || S->epoch != seen; };
+            if (S->hold_until == Clock::time_point::max())
+                S->cv_work.wait(lk, ready);
+            else
+                S->cv_work.wait_until(lk, S->hold_until, ready);
             seen = S->epoch;
             S->nbox_seen = (int)S->boxes.size();
             while (!S->incoming.empty()) {
@@ -774,7 +816,13 @@ void dispatcher(p2p_server *S) {
                 if (L->kernel_seen && L->copy_done) cdone.push_back(L);
             }
             stopping = S->stop;
+            if (S->set_window_ms >= 0.0) {
+                S->cfg.batch_window_ms = S->set_window_ms;
+                S->cfg.min_pack_pairs = S->set_min_pairs;
+                S->set_window_ms = -1.0;
+            }
         }
+        S->flush = stopping;
         int st = P2P_OK;
         for (Launch *L : kdone)
             if (st == P2P_OK) st = retire_kernel(S, *L);
@@ -879,6 +927,10 @@ P2P_API int p2p_server_create(int device, const p2p_params *shape, const p2p_ser
         c.full_grid = cfg->full_grid;
         c.hbm_bytes = cfg->hbm_bytes;
         if (cfg->rows_per_particle > 0) c.rows_per_particle = cfg->rows_per_particle;
+        if (!(cfg->batch_window_ms >= 0.0) || !(cfg->min_pack_pairs >= 0.0) || cfg->batch_window_ms > 1e4)
+            return fail(P2P_ERR_ARG, "batch_window_ms must be in [0, 1e4] and min_pack_pairs >= 0");
+        c.batch_window_ms = cfg->batch_window_ms;
+        c.min_pack_pairs = cfg->min_pack_pairs;
         if (cfg->particles_per_leaf > 0) c.particles_per_leaf = std::max(1.0, cfg->particles_per_leaf);
     }
     p2p_server *S = new p2p_server();
@@ -1059,7 +1111,7 @@ P2P_API int p2p_server_submit(p2p_server *S, int box_id, double *out, int64_t *t
         r.t_submit = now;
         *ticket = (int64_t)S->reqs.size();
         S->reqs.push_back(r);
-        S->incoming.push_back(Job{*ticket, box_id, out, false});
+        S->incoming.push_back(Job{*ticket, box_id, out, false, now});
         S->submitted++;
     }
     S->cv_work.notify_all();
@@ -1078,7 +1130,7 @@ P2P_API int p2p_server_preload(p2p_server *S, int box_id) {
         r.t_submit = Clock::now();
         ticket = (int64_t)S->reqs.size();
         S->reqs.push_back(r);
-        S->incoming.push_back(Job{ticket, box_id, nullptr, true});
+        S->incoming.push_back(Job{ticket, box_id, nullptr, true, r.t_submit});
         S->submitted++;
     }
     S->cv_work.notify_all();
@@ -1108,6 +1160,20 @@ P2P_API int p2p_server_wait(p2p_server *S, int64_t ticket, double *latency_s) {
         return fail(S->error, "server failed: %s", S->error_msg.c_str());
     if (r.status != P2P_OK) return fail(r.status, "request %lld: box does not fit in the arena", (long long)ticket);
     if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
+    return P2P_OK;
+}
+
+P2P_API int p2p_server_set_batching(p2p_server *S, double batch_window_ms, double min_pack_pairs) {
+    if (!S) return fail(P2P_ERR_ARG, "null server");
+    if (!(batch_window_ms >= 0.0) || batch_window_ms > 1e4 || !(min_pack_pairs >= 0.0))
+        return fail(P2P_ERR_ARG, "batch_window_ms must be in [0, 1e4] and min_pack_pairs >= 0");
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        S->set_window_ms = batch_window_ms;
+        S->set_min_pairs = min_pack_pairs;
+        S->epoch++;
+    }
+    S->cv_work.notify_all();
     return P2P_OK;
 }
 

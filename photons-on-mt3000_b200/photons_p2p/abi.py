@@ -57,6 +57,8 @@ class ServerConfig(ctypes.Structure):
         ("hbm_bytes", ctypes.c_size_t),
         ("rows_per_particle", ctypes.c_double),
         ("particles_per_leaf", ctypes.c_double),
+        ("batch_window_ms", ctypes.c_double),
+        ("min_pack_pairs", ctypes.c_double),
     ]
 
 
@@ -144,6 +146,7 @@ SIGNATURES = {
     "p2p_server_wait": (_i, [_vp, _i64, ctypes.POINTER(_d)]),
     "p2p_server_query": (_i, [_vp, _i64, ctypes.POINTER(_i), ctypes.POINTER(_d)]),
     "p2p_server_drain": (_i, [_vp]),
+    "p2p_server_set_batching": (_i, [_vp, _d, _d]),
     "p2p_server_get_stats": (_i, [_vp, ctypes.POINTER(ServerStats)]),
     "p2p_dtree_build": (_i, [_vp, _i, _vp, _vp, _i, _d, ctypes.POINTER(_vp)]),
     "p2p_dtree_free": (_i, [_vp]),

@@ -57,7 +57,7 @@ class BoxEntry:
 
 class Server:
     def __init__(self, shape, device=0, slots=1, max_pack=32, full_grid=True, hbm_bytes=0,
-                 rows_per_particle=0.0, particles_per_leaf=0.0):
+                 rows_per_particle=0.0, particles_per_leaf=0.0, batch_window_ms=0.0, min_pack_pairs=0.0):
         self.lib = _native.core()
         cfg = ServerConfig()
         self.lib.p2p_server_config_default(ctypes.byref(cfg))
@@ -69,12 +69,20 @@ class Server:
             cfg.rows_per_particle = rows_per_particle
         if particles_per_leaf:
             cfg.particles_per_leaf = particles_per_leaf
+        cfg.batch_window_ms = batch_window_ms
+        cfg.min_pack_pairs = min_pack_pairs
         h = ctypes.c_void_p()
         _check(self.lib, self.lib.p2p_server_create(device, ctypes.byref(shape), ctypes.byref(cfg),
                                                     ctypes.byref(h)))
         self.h = h
         self.boxes = []
         self.inflight = {}   # ticket -> (box index, PinnedArray)
+
+    def set_batching(self, batch_window_ms, min_pack_pairs=0.0):
+        """Batching window: pending requests wait up to batch_window_ms for
+        others to share their launch unless the pack already holds max_pack
+        boxes or min_pack_pairs pair interactions (0 ms: launch at once)."""
+        _check(self.lib, self.lib.p2p_server_set_batching(self.h, float(batch_window_ms), float(min_pack_pairs)))
 
     def close(self):
         if self.h:

@@ -207,3 +207,37 @@ def test_box_larger_than_arena(gpu, ensemble):
         with pytest.raises(P2PError) as ei:
             srv.add_box(lists[k], 0.5 / boxes[k].cfg.split_radius, 1.0)
         assert ei.value.status == abi.P2P_ERR_CAPACITY
+
+
+@pytest.mark.gpu
+def test_batching_window_packs_and_keeps_results(gpu, ensemble):
+    """With a batching window, requests submitted one after another within
+    it share one launch, each result equals the box computed alone, a lone
+    request waits out the window, and min_pack_pairs launches a pack at once."""
+    import time
+
+    with make_server(abi.FORM_SPLIT, ensemble, device=gpu, slots=1) as srv:
+        ref = [alone(srv, k) for k in range(4)]
+        srv.set_batching(400.0)
+        s0 = srv.stats()
+        tickets = []
+        for k in range(4):
+            tickets.append(srv.submit(k))
+            time.sleep(0.01)
+        for k, t in enumerate(tickets):
+            out, lat = srv.wait(t)
+            assert rel_err(out, ref[k])[1] <= MIX_TOL
+        s1 = srv.stats()
+        assert s1["launches"] - s0["launches"] == 1
+        assert s1["boxes_launched"] - s0["boxes_launched"] == 4
+        # a lone request of a resident box waits out the window (a box not yet
+        # built has no pair count and launches at once)
+        _, lat = srv.wait(srv.submit(0))
+        assert lat >= 0.4
+        # one request of any size reaches a 1-pair threshold: no waiting
+        srv.set_batching(5000.0, 1.0)
+        _, lat = srv.wait(srv.submit(1))
+        assert lat < 2.0
+        srv.set_batching(0.0)
+        with pytest.raises(P2PError):
+            srv.set_batching(-1.0)
