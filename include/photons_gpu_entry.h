@@ -48,7 +48,10 @@ double get_last_kntime(int proc_rank);
 
 /* Result staging and acc[d][i] += result for the particles of the packs
  * (active_level -1: all). Replace src/gpu_func.impl.h:264-275, :644-681
- * (src/gravity.c:317-319, :444-446). packs is the reference's P2PPack array. */
+ * (src/gravity.c:317-319, :444-446). packs is the reference's P2PPack array.
+ * The staging is the module's page-locked buffer, kept between passes (one
+ * pinned D2H per pass, no allocation); hostfree_out only releases the
+ * reservation, devfree the memory. */
 void hostmalloc_out(int npart);
 void devMemcpyDH_updateAcc(void *packs, int npack, int active_level);
 void hostfree_out(void);
@@ -62,6 +65,13 @@ void dinfofree(void);
 /* Waits for all queued device work. Replaces sync_with_dev,
  * src/gpu_func.impl.h:133-135. */
 void sync_with_dev(void);
+
+/* Position bytes the last pass uploaded (no counterpart in the reference).
+ * The module keeps the previous pass's packed positions in its page-locked
+ * staging and on the device; a pass uploads only the 65536-particle chunks
+ * whose positions changed, so a pass over unmoved particles uploads none. */
+#include <stdint.h>
+int64_t p2p_dropin_last_upload_bytes(void);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,19 @@ double p2p_session_poly_error(const p2p_session *s);
  * ints, each leaf a range of particle slots [ipart, ipart+npart). */
 int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *masses,
                    int nleaf, const int *leaf_ipart, const int *leaf_npart);
+/* p2p_pass_begin with equal masses for positions that mostly equal the
+ * previous pass's: the session keeps the positions of its last host-input
+ * begin on the device, and only the chunks flagged in dirty (chunk c holds
+ * particles [c*chunk, (c+1)*chunk), all three coordinate rows) are uploaded.
+ * The caller guarantees that unflagged chunks equal what it passed before.
+ * Every chunk is uploaded when dirty is NULL, when npart differs from the
+ * previous host-input pass, or when the session's buffers had to grow.
+ * uploaded_bytes (nullable) receives the bytes queued. The device half of
+ * PhotoNs' per-pass particle upload (src/gpu_entry.cu:82-122) made
+ * incremental; no counterpart in the reference. */
+int p2p_pass_begin_update(p2p_session *s, int npart, const double *pos, int nleaf, const int *leaf_ipart,
+                          const int *leaf_npart, const unsigned char *dirty, int64_t chunk,
+                          int64_t *uploaded_bytes);
 /* Same with device pointers (already resident in HBM; not copied). */
 int p2p_pass_begin_device(p2p_session *s, int npart, const double *d_pos, const double *d_masses,
                           int nleaf, const int *d_leaf_ipart, const int *d_leaf_npart);

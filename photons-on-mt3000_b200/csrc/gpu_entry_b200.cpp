@@ -8,9 +8,11 @@
 // The functions read the same globals the reference's versions read and keep
 // its call protocol, ownership and print-and-exit error behaviour; the
 // declarations are listed in include/photons_gpu_entry.h.
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 extern "C" {
 #include "photoNs.h"
@@ -25,6 +27,7 @@ long long g_tot_tasks = 0;
 bool g_pass_open = false;
 double *g_out = nullptr;  // h_part_buf of the reference
 int g_out_n = 0;
+int64_t g_uploaded = 0;   // position bytes the last pass uploaded
 
 void check(const char *where, int status);
 
@@ -52,7 +55,12 @@ struct Pinned {
         cap = 0;
     }
 };
-Pinned g_pin_pos, g_pin_leaf, g_pin_tasks;
+Pinned g_pin_pos, g_pin_leaf, g_pin_tasks, g_pin_out;
+// Particles whose packed positions g_pin_pos holds from the previous pass
+// (-1: none): the next pass compares while packing and uploads only the
+// chunks that changed (p2p_pass_begin_update).
+int g_pin_pos_n = -1;
+constexpr int kDirtyChunk = 1 << 16;
 
 [[noreturn]] void die(const char *where, int status) {
     // checkDevErrors, src/gpu_func.impl.h:70-86
@@ -111,31 +119,55 @@ void set_pass_params() {
 }
 
 // SoA pack of the particle positions (src/gpu_entry.cu:85-105) and the leaf
-// table (:108-111), then the first-call upload (devMemcpyHD_part).
+// table (:108-111), then the first-call upload (devMemcpyHD_part). The pack
+// goes into the module's page-locked staging, which keeps the previous
+// pass's positions: each chunk of 65536 particles is compared (bit for bit)
+// while it is packed, and only chunks that changed are uploaded over the
+// copy the session keeps on the device.
 void begin_pass() {
     init_device();
     set_pass_params();
     const int n = NPART;
     const int nleaf = last_leaf - first_leaf;
+    const void *before = g_pin_pos.p;
     double *pos = (double *)g_pin_pos.get(sizeof(double) * 3 * (size_t)(n > 0 ? n : 1));
-    // (the reference packs on one thread; the iterations are independent)
+    const bool have_old = g_pin_pos_n == n && pos == before;
+    const int nchunk = (n + kDirtyChunk - 1) / kDirtyChunk;
+    std::vector<unsigned char> dirty((size_t)(nchunk > 0 ? nchunk : 1), have_old ? 0 : 1);
+    // (the reference packs on one thread; the chunks are independent)
 #pragma omp parallel for schedule(static)
-    for (int i = 0; i < n; ++i) {
-        for (int d = 0; d < 3; ++d) {
+    for (int c = 0; c < nchunk; ++c) {
+        const int i1 = (c + 1) * kDirtyChunk < n ? (c + 1) * kDirtyChunk : n;
+        unsigned char changed = 0;
+        for (int i = c * kDirtyChunk; i < i1; ++i) {
+            for (int d = 0; d < 3; ++d) {
 #ifndef INTXYZ
-            pos[(size_t)d * n + i] = part[i].pos[d];
+                const double v = part[i].pos[d];
 #else
-            pos[(size_t)d * n + i] = INT2POS * (part[i].posi[d] - domain_center_i[d]);
+                const double v = INT2POS * (part[i].posi[d] - domain_center_i[d]);
 #endif
+                double &slot = pos[(size_t)d * n + i];
+                if (have_old) {
+                    uint64_t a, b;
+                    std::memcpy(&a, &slot, 8);
+                    std::memcpy(&b, &v, 8);
+                    changed |= (unsigned char)(a != b);
+                }
+                slot = v;
+            }
         }
+        if (have_old) dirty[(size_t)c] = changed;
     }
+    g_pin_pos_n = -1;
     int *ip = (int *)g_pin_leaf.get(sizeof(int) * 2 * (size_t)(nleaf > 0 ? nleaf : 1));
     int *np = ip + nleaf;
     for (int l = 0; l < nleaf; ++l) {
         ip[l] = leaf[l + first_leaf].ipart;
         np[l] = leaf[l + first_leaf].npart;
     }
-    check("p2p_pass_begin", p2p_pass_begin(g_sess, n, pos, nullptr, nleaf, ip, np));
+    check("p2p_pass_begin_update",
+          p2p_pass_begin_update(g_sess, n, pos, nleaf, ip, np, dirty.data(), kDirtyChunk, &g_uploaded));
+    g_pin_pos_n = n;
     g_pass_open = true;
 }
 
@@ -230,13 +262,15 @@ double get_last_kntime(int proc_rank) {
     return sec;
 }
 
+// The result buffer is the module's page-locked staging (grow-only, kept
+// until devfree), so the D2H is one pinned copy and no allocation per pass;
+// these two only mark it reserved, as the reference's malloc / free did.
 void hostmalloc_out(int npart) {
-    g_out = (double *)malloc(sizeof(double) * 3 * (size_t)(npart > 0 ? npart : 1));
+    g_out = (double *)g_pin_out.get(sizeof(double) * 3 * (size_t)(npart > 0 ? npart : 1));
     g_out_n = npart;
 }
 
 void hostfree_out(void) {
-    free(g_out);
     g_out = nullptr;
     g_out_n = 0;
 }
@@ -303,12 +337,18 @@ void devfree(void) {
     g_pin_pos.release();
     g_pin_leaf.release();
     g_pin_tasks.release();
+    g_pin_out.release();
+    g_pin_pos_n = -1;
+    g_out = nullptr;
+    g_out_n = 0;
     g_pass_open = false;
     g_call_cnt = 0;
     g_tot_tasks = 0;
 }
 
 void dinfofree(void) {}
+
+int64_t p2p_dropin_last_upload_bytes(void) { return g_uploaded; }
 
 void sync_with_dev(void) {
     if (g_sess) check("p2p_session_synchronize", p2p_session_synchronize(g_sess));

@@ -92,6 +92,10 @@ struct p2p_session {
     // pass state
     bool in_pass = false;
     int npart = 0, nleaf = 0;
+    // particles whose host positions the pos buffer holds from the last
+    // p2p_pass_begin / p2p_pass_begin_update (-1: none); p2p_pass_begin_update
+    // uploads only the changed chunks over them
+    int pos_held = -1;
     const double *d_pos = nullptr, *d_mass = nullptr;
     const int *d_ip = nullptr, *d_np = nullptr;
     // graph cache for p2p_pass_run_device
@@ -547,8 +551,9 @@ P2P_API int p2p_session_poly_degree(const p2p_session *s) { return s ? s->fit.de
 
 P2P_API double p2p_session_poly_error(const p2p_session *s) { return s ? s->fit.max_err : 0.0; }
 
-P2P_API int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *masses,
-                           int nleaf, const int *leaf_ipart, const int *leaf_npart) {
+namespace {
+int check_host_begin(p2p_session *s, int npart, const double *pos, int nleaf, const int *leaf_ipart,
+                     const int *leaf_npart) {
     P2P_TRY(check_session(s));
     if (s->in_pass) return fail(P2P_ERR_STATE, "pass already open");
     if (npart < 0 || nleaf < 0) return fail(P2P_ERR_ARG, "negative size");
@@ -560,17 +565,19 @@ P2P_API int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const d
             return fail(P2P_ERR_RANGE, "leaf %d covers [%lld, %lld) outside [0, %d)", l,
                         (long long)ip, (long long)(ip + np), npart);
     }
-    P2P_TRY(size_pass_buffers(s, npart, nleaf, true, masses != nullptr));
-    s->npart = npart;
-    s->nleaf = nleaf;
-    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
-    if (npart) CUDA_TRY(cudaMemcpyAsync(s->pos.p, pos, sizeof(double) * 3 * (size_t)npart, cudaMemcpyHostToDevice, s->stream));
+    return P2P_OK;
+}
+
+// The leaf table upload and the pass state after the positions are queued.
+int finish_host_begin(p2p_session *s, int npart, const double *masses, int nleaf, const int *leaf_ipart,
+                      const int *leaf_npart) {
     if (masses && npart)
         CUDA_TRY(cudaMemcpyAsync(s->mass.p, masses, sizeof(double) * (size_t)npart, cudaMemcpyHostToDevice, s->stream));
     if (nleaf) {
         CUDA_TRY(cudaMemcpyAsync(s->leaf_ip.p, leaf_ipart, sizeof(int) * (size_t)nleaf, cudaMemcpyHostToDevice, s->stream));
         CUDA_TRY(cudaMemcpyAsync(s->leaf_np.p, leaf_npart, sizeof(int) * (size_t)nleaf, cudaMemcpyHostToDevice, s->stream));
     }
+    s->pos_held = npart;
     s->d_pos = (const double *)s->pos.p;
     s->d_mass = masses ? (const double *)s->mass.p : nullptr;
     s->d_ip = (const int *)s->leaf_ip.p;
@@ -579,6 +586,59 @@ P2P_API int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const d
     s->in_pass = true;
     s->kernel_timed = false;
     return P2P_OK;
+}
+}  // namespace
+
+P2P_API int p2p_pass_begin(p2p_session *s, int npart, const double *pos, const double *masses,
+                           int nleaf, const int *leaf_ipart, const int *leaf_npart) {
+    P2P_TRY(check_host_begin(s, npart, pos, nleaf, leaf_ipart, leaf_npart));
+    s->pos_held = -1;
+    P2P_TRY(size_pass_buffers(s, npart, nleaf, true, masses != nullptr));
+    s->npart = npart;
+    s->nleaf = nleaf;
+    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
+    if (npart) CUDA_TRY(cudaMemcpyAsync(s->pos.p, pos, sizeof(double) * 3 * (size_t)npart, cudaMemcpyHostToDevice, s->stream));
+    return finish_host_begin(s, npart, masses, nleaf, leaf_ipart, leaf_npart);
+}
+
+P2P_API int p2p_pass_begin_update(p2p_session *s, int npart, const double *pos, int nleaf, const int *leaf_ipart,
+                                  const int *leaf_npart, const unsigned char *dirty, int64_t chunk,
+                                  int64_t *uploaded_bytes) {
+    P2P_TRY(check_host_begin(s, npart, pos, nleaf, leaf_ipart, leaf_npart));
+    if (dirty && chunk <= 0) return fail(P2P_ERR_ARG, "chunk must be positive");
+    const void *before = s->pos.p;
+    const bool held = s->pos_held == npart;
+    s->pos_held = -1;
+    P2P_TRY(size_pass_buffers(s, npart, nleaf, true, false));
+    s->npart = npart;
+    s->nleaf = nleaf;
+    CUDA_TRY(cudaEventRecord(s->ev_begin, s->stream));
+    const size_t n = (size_t)npart;
+    double *dst = (double *)s->pos.p;
+    int64_t bytes = 0;
+    if (!dirty || !held || s->pos.p != before) {
+        if (npart) CUDA_TRY(cudaMemcpyAsync(dst, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s->stream));
+        bytes = (int64_t)(sizeof(double) * 3 * n);
+    } else {
+        // runs of changed chunks, one copy per coordinate row and run
+        const int64_t nchunk = (npart + chunk - 1) / chunk;
+        for (int64_t c = 0; c < nchunk;) {
+            if (!dirty[c]) {
+                ++c;
+                continue;
+            }
+            int64_t e = c;
+            while (e < nchunk && dirty[e]) ++e;
+            const size_t a = (size_t)(c * chunk), b = std::min(n, (size_t)(e * chunk));
+            for (int d = 0; d < 3; ++d)
+                CUDA_TRY(cudaMemcpyAsync(dst + d * n + a, pos + d * n + a, sizeof(double) * (b - a),
+                                         cudaMemcpyHostToDevice, s->stream));
+            bytes += (int64_t)(3 * sizeof(double) * (b - a));
+            c = e;
+        }
+    }
+    if (uploaded_bytes) *uploaded_bytes = bytes;
+    return finish_host_begin(s, npart, nullptr, nleaf, leaf_ipart, leaf_npart);
 }
 
 P2P_API int p2p_pass_begin_device(p2p_session *s, int npart, const double *d_pos,

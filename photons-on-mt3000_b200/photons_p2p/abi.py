@@ -116,6 +116,7 @@ SIGNATURES = {
     "p2p_session_poly_degree": (_i, [_vp]),
     "p2p_session_poly_error": (_d, [_vp]),
     "p2p_pass_begin": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
+    "p2p_pass_begin_update": (_i, [_vp, _i, _vp, _i, _vp, _vp, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "p2p_pass_begin_device": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp]),
     "p2p_pass_submit": (_i, [_vp, _i64, _vp, _vp]),
     "p2p_pass_submit_device": (_i, [_vp, _i64, _vp, _vp]),
