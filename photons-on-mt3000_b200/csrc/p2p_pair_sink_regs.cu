@@ -42,8 +42,14 @@ cudaError_t allow_one() {
                         (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 17>,
                         (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 21>};
     cudaError_t e = cudaSuccess;
-    for (const void *k : ks)
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    for (const void *k : ks) {
+        // the opt-in limit covers static and dynamic shared memory together
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024 - (int)fa.sharedSizeBytes);
+    }
     return e;
 }
 
