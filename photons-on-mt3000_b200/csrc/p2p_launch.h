@@ -49,8 +49,11 @@ inline size_t pair_smem_sx2(int warps, int stage) { return (size_t)warps * (stag
 // accumulators + staging context; its stage holds at least kSregMinStage sources (one staging group)
 constexpr int kSregMinStage = 128;
 inline int sreg_stage(int stage) { return stage < kSregMinStage ? kSregMinStage : stage; }
+#ifndef P2P_SREG_SPL
+#define P2P_SREG_SPL 4  // sinks per lane of the sink-register kernel
+#endif
 inline size_t pair_smem_sreg(int warps, int stage) {
-    return (size_t)warps * ((size_t)sreg_stage(stage) * 32 + 12 * 32 * 8 + 1024);
+    return (size_t)warps * ((size_t)sreg_stage(stage) * 32 + 3 * P2P_SREG_SPL * 32 * 8 + 1024);
 }
 
 // Persistent grid for `kernel`: blocks_per_sm, or as many as registers and

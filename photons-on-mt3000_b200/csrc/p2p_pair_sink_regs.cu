@@ -12,12 +12,12 @@ PairLaunchResult by_ncoef(const PairLaunch &L0, const PairArgs &a) {
     L.stage = sreg_stage(L0.stage);  // the kernel's stage capacity (at least one staging group)
     const size_t smem = pair_smem_sreg(L.warps, L.stage);
     switch (L.ncoef) {
-        case 9: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 9>, smem, a);
-        case 11: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 11>, smem, a);
-        case 13: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 13>, smem, a);
-        case 15: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 15>, smem, a);
-        case 17: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 17>, smem, a);
-        case 21: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 21>, smem, a);
+        case 9: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 9, P2P_SREG_SPL>, smem, a);
+        case 11: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 11, P2P_SREG_SPL>, smem, a);
+        case 13: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 13, P2P_SREG_SPL>, smem, a);
+        case 15: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 15, P2P_SREG_SPL>, smem, a);
+        case 17: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 17, P2P_SREG_SPL>, smem, a);
+        case 21: return launch_persistent(L, pair_sreg_kernel<SOFT, MASSES, ACC, 21, P2P_SREG_SPL>, smem, a);
         default: {
             PairLaunchResult r;
             r.cuda = cudaErrorInvalidValue;
@@ -35,12 +35,12 @@ PairLaunchResult by_soft(const PairLaunch &L, const PairArgs &a) {
 
 template <int SOFT, bool MASSES, int ACC>
 cudaError_t allow_one() {
-    const void *ks[] = {(const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 9>,
-                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 11>,
-                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 13>,
-                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 15>,
-                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 17>,
-                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 21>};
+    const void *ks[] = {(const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 9, P2P_SREG_SPL>,
+                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 11, P2P_SREG_SPL>,
+                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 13, P2P_SREG_SPL>,
+                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 15, P2P_SREG_SPL>,
+                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 17, P2P_SREG_SPL>,
+                        (const void *)pair_sreg_kernel<SOFT, MASSES, ACC, 21, P2P_SREG_SPL>};
     cudaError_t e = cudaSuccess;
     for (const void *k : ks) {
         // the opt-in limit covers static and dynamic shared memory together

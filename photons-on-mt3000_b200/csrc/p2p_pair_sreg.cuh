@@ -1,12 +1,14 @@
 // Sink-register pair kernel of the FP32 forms (P2P_VARIANT_SINK_REGS).
 //
 // A slice of ns <= 32 sink particles of a sink leaf is split into G =
-// ceil(ns / 4) groups of four; lane (g, j) = (lane % G, lane / G), j < J =
-// floor(32 / G), keeps group g's four sinks in registers as two packed sink
-// pairs and takes the staged sources j, j + J, j + 2J, ... of the row. A
-// staged source is read as two 16-byte shared-memory loads (stored
-// pre-duplicated: (x, x, y, y), (z, z, w, index)) and evaluated against the
-// four sinks with sm_100's packed FP32 instructions (pair_split_x2): no
+// ceil(ns / SPL) groups of SPL sinks (SPL = P2P_SREG_SPL, 4; 8 was measured
+// slower: 168 registers, 3 blocks per SM, more padded sinks); lane (g, j) =
+// (lane % G, lane / G), j < J = floor(32 / G), keeps group g's sinks in
+// registers as SPL / 2 packed sink pairs and takes the staged sources j,
+// j + J, j + 2J, ... of the row. A staged source is read as two 16-byte
+// shared-memory loads (stored pre-duplicated: (x, x, y, y), (z, z, w,
+// index)) and evaluated against the lane's sinks with sm_100's packed FP32
+// instructions (pair_split_x2n): no
 // per-pair shared loads of sinks, no predicated sink blocks, so the FP32 pipe
 // rather than instruction issue bounds the loop.
 //
@@ -76,7 +78,8 @@ template <> struct SregAcc<ACC_F32> {
 constexpr int kSregRounds = P2P_SREG_ROUNDS;
 static_assert(32 * kSregRounds <= kSregMinStage, "a staging group must fit in the smallest stage");
 
-constexpr int kSregAccBytes = 12 * 32 * 8;  // 12 values per lane, at most 8 bytes each
+// 3 values per sink per lane, at most 8 bytes each
+__host__ __device__ constexpr int sreg_acc_bytes(int spl) { return 3 * spl * 32 * 8; }
 
 // Staging context of one warp, kept in shared memory rather than registers
 // so that none of it is live while the warp evaluates pairs: the current
@@ -95,45 +98,46 @@ static_assert(sizeof(SregCtx) <= kSregCtxBytes, "staging context");
 
 // Shared memory of one warp: staged sources (32 B each), the lane
 // accumulators, the staging context.
-__host__ __device__ constexpr size_t sreg_warp_bytes(int cap) {
-    return (size_t)cap * 32 + kSregAccBytes + kSregCtxBytes;
+__host__ __device__ constexpr size_t sreg_warp_bytes(int cap, int spl) {
+    return (size_t)cap * 32 + sreg_acc_bytes(spl) + kSregCtxBytes;
 }
 
-// The lane's four sinks as two packed pairs and their FP32 partial forces.
+// The lane's SPL sinks as SPL / 2 packed pairs and their FP32 partial forces.
+template <int SPL>
 struct SregLane {
-    float2 pax, pay, paz, pbx, pby, pbz;  // negated coordinates of sinks (4g, 4g+1) and (4g+2, 4g+3)
-    float2 ax, ay, az, bx, by, bz;        // partials of the two pairs
-    int sfirst, slast;                    // particle index of sink 4g, and of the slice's last sink
+    static constexpr int P = SPL / 2;
+    float2 px[P], py[P], pz[P];  // negated coordinates of sinks (SPL g + 2 p, SPL g + 2 p + 1)
+    float2 ax[P], ay[P], az[P];  // partials of the pairs
+    int sfirst, slast;           // particle index of sink SPL g, and of the slice's last sink
 };
 
-// One staged source (pre-duplicated layout) against the lane's four sinks.
-template <int SOFT, bool MASSES, int NC, bool CHECK>
-__device__ __forceinline__ void sreg_eval(const float4 A, const float4 B, SregLane &L, const PairArgs &a,
+// One staged source (pre-duplicated layout) against the lane's sinks.
+template <int SOFT, bool MASSES, int NC, bool CHECK, int SPL>
+__device__ __forceinline__ void sreg_eval(const float4 A, const float4 B, SregLane<SPL> &L, const PairArgs &a,
                                           const float2 eps2v, const float2 negu0v, bool &amb) {
     const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w), sz = make_float2(B.x, B.y);
-    pair_split_x2n<SOFT, MASSES, NC, CHECK>(sx, sy, sz, B.z, L.pax, L.pay, L.paz, a, eps2v, negu0v, L.ax, L.ay, L.az,
-                                            amb);
-    pair_split_x2n<SOFT, MASSES, NC, CHECK>(sx, sy, sz, B.z, L.pbx, L.pby, L.pbz, a, eps2v, negu0v, L.bx, L.by, L.bz,
-                                            amb);
+#pragma unroll
+    for (int p = 0; p < SPL / 2; ++p)
+        pair_split_x2n<SOFT, MASSES, NC, CHECK>(sx, sy, sz, B.z, L.px[p], L.py[p], L.pz[p], a, eps2v, negu0v,
+                                                L.ax[p], L.ay[p], L.az[p], amb);
 }
 
 // Re-decides the lane's band pairs with one staged source from FP64 positions.
-template <int SOFT, bool MASSES, int NC>
-__device__ __forceinline__ void sreg_band(const float4 A, const float4 B, SregLane &L, const PairArgs &a) {
+template <int SOFT, bool MASSES, int NC, int SPL>
+__device__ __forceinline__ void sreg_band(const float4 A, const float4 B, SregLane<SPL> &L, const PairArgs &a) {
     const float4 src = make_float4(A.x, A.z, B.x, B.z);
     const int isrc = __float_as_int(B.w);
     float3 cb;
-    if (band_pair<SOFT, MASSES, NC>(src, L.pax.x, L.pay.x, L.paz.x, isrc, L.sfirst, a, &cb)) {
-        L.ax.x += cb.x; L.ay.x += cb.y; L.az.x += cb.z;
-    }
-    if (band_pair<SOFT, MASSES, NC>(src, L.pax.y, L.pay.y, L.paz.y, isrc, min(L.sfirst + 1, L.slast), a, &cb)) {
-        L.ax.y += cb.x; L.ay.y += cb.y; L.az.y += cb.z;
-    }
-    if (band_pair<SOFT, MASSES, NC>(src, L.pbx.x, L.pby.x, L.pbz.x, isrc, min(L.sfirst + 2, L.slast), a, &cb)) {
-        L.bx.x += cb.x; L.by.x += cb.y; L.bz.x += cb.z;
-    }
-    if (band_pair<SOFT, MASSES, NC>(src, L.pbx.y, L.pby.y, L.pbz.y, isrc, min(L.sfirst + 3, L.slast), a, &cb)) {
-        L.bx.y += cb.x; L.by.y += cb.y; L.bz.y += cb.z;
+#pragma unroll
+    for (int p = 0; p < SPL / 2; ++p) {
+        if (band_pair<SOFT, MASSES, NC>(src, L.px[p].x, L.py[p].x, L.pz[p].x, isrc, min(L.sfirst + 2 * p, L.slast),
+                                        a, &cb)) {
+            L.ax[p].x += cb.x; L.ay[p].x += cb.y; L.az[p].x += cb.z;
+        }
+        if (band_pair<SOFT, MASSES, NC>(src, L.px[p].y, L.py[p].y, L.pz[p].y, isrc,
+                                        min(L.sfirst + 2 * p + 1, L.slast), a, &cb)) {
+            L.ax[p].y += cb.x; L.ay[p].y += cb.y; L.az[p].y += cb.z;
+        }
     }
 }
 
@@ -142,9 +146,9 @@ __device__ __forceinline__ void sreg_band(const float4 A, const float4 B, SregLa
 // without per-lane guards; with tail the last, partial iteration follows,
 // guarded per lane. Returns the sources consumed (n with tail, else the
 // whole iterations' 2 J k).
-template <int SOFT, bool MASSES, int NC, bool CHECK>
+template <int SOFT, bool MASSES, int NC, bool CHECK, int SPL>
 __device__ __forceinline__ int sreg_region(const float4 *stage, const int base, const int n, const int j, const int J,
-                                           const bool owner, const bool tail, SregLane &L, const PairArgs &a,
+                                           const bool owner, const bool tail, SregLane<SPL> &L, const PairArgs &a,
                                            const float2 eps2v, const float2 negu0v) {
     const int step = 2 * J;
     const int full = n / step;
@@ -157,8 +161,8 @@ __device__ __forceinline__ int sreg_region(const float4 *stage, const int base, 
             const float4 A0 = p[0], B0 = p[1], A1 = p[2 * J], B1 = p[2 * J + 1];
             p += 2 * step;
             bool amb = false;
-            sreg_eval<SOFT, MASSES, NC, CHECK>(A0, B0, L, a, eps2v, negu0v, amb);
-            sreg_eval<SOFT, MASSES, NC, CHECK>(A1, B1, L, a, eps2v, negu0v, amb);
+            sreg_eval<SOFT, MASSES, NC, CHECK, SPL>(A0, B0, L, a, eps2v, negu0v, amb);
+            sreg_eval<SOFT, MASSES, NC, CHECK, SPL>(A1, B1, L, a, eps2v, negu0v, amb);
             if (CHECK) ambbits |= amb ? (1u << k) : 0u;
         }
         if (CHECK && owner) {
@@ -166,8 +170,8 @@ __device__ __forceinline__ int sreg_region(const float4 *stage, const int base, 
                 const int k = __ffs(ambbits) - 1;
                 ambbits &= ambbits - 1;
                 const int s = base + j + (ib + k) * step;
-                sreg_band<SOFT, MASSES, NC>(stage[2 * s], stage[2 * s + 1], L, a);
-                sreg_band<SOFT, MASSES, NC>(stage[2 * (s + J)], stage[2 * (s + J) + 1], L, a);
+                sreg_band<SOFT, MASSES, NC, SPL>(stage[2 * s], stage[2 * s + 1], L, a);
+                sreg_band<SOFT, MASSES, NC, SPL>(stage[2 * (s + J)], stage[2 * (s + J) + 1], L, a);
             }
         }
     }
@@ -180,8 +184,8 @@ __device__ __forceinline__ int sreg_region(const float4 *stage, const int base, 
             const int s = base + k;
             const float4 A = stage[2 * s], B = stage[2 * s + 1];
             bool amb = false;
-            sreg_eval<SOFT, MASSES, NC, CHECK>(A, B, L, a, eps2v, negu0v, amb);
-            if (CHECK && owner && amb) sreg_band<SOFT, MASSES, NC>(A, B, L, a);
+            sreg_eval<SOFT, MASSES, NC, CHECK, SPL>(A, B, L, a, eps2v, negu0v, amb);
+            if (CHECK && owner && amb) sreg_band<SOFT, MASSES, NC, SPL>(A, B, L, a);
         }
     }
     return n;
@@ -193,39 +197,40 @@ __device__ __forceinline__ int sreg_region(const float4 *stage, const int base, 
 // region's bottom, so each remainder stays where the next sources join it
 // ([0, ni) and [cap - nc, cap) again). The FP32 partials go into the lane's
 // shared-memory accumulators.
-template <int SOFT, bool MASSES, int ACC, int NC>
+template <int SOFT, bool MASSES, int ACC, int NC, int SPL>
 __device__ __forceinline__ void sreg_consume(const float4 *stage, typename SregAcc<ACC>::T *accs, const int cap,
                                              int &ni, int &nc, const bool fin, const int j, const int J,
-                                             const bool owner, SregLane &L, const PairArgs &a, const float2 eps2v,
+                                             const bool owner, SregLane<SPL> &L, const PairArgs &a, const float2 eps2v,
                                              const float2 negu0v) {
     using SA = SregAcc<ACC>;
     const int lane = threadIdx.x & 31;
     __syncwarp();
     const int rin = fin ? 0 : ni % (2 * J);  // inside sources left for the next consume
-    sreg_region<SOFT, MASSES, NC, false>(stage, rin, ni - rin, j, J, owner, fin, L, a, eps2v, negu0v);
+    sreg_region<SOFT, MASSES, NC, false, SPL>(stage, rin, ni - rin, j, J, owner, fin, L, a, eps2v, negu0v);
     ni = rin;
-    nc -= sreg_region<SOFT, MASSES, NC, true>(stage, cap - nc, nc, j, J, owner, fin, L, a, eps2v, negu0v);
-    SA::add(accs[0 * 32 + lane], L.ax.x); SA::add(accs[1 * 32 + lane], L.ay.x);
-    SA::add(accs[2 * 32 + lane], L.az.x); SA::add(accs[3 * 32 + lane], L.ax.y);
-    SA::add(accs[4 * 32 + lane], L.ay.y); SA::add(accs[5 * 32 + lane], L.az.y);
-    SA::add(accs[6 * 32 + lane], L.bx.x); SA::add(accs[7 * 32 + lane], L.by.x);
-    SA::add(accs[8 * 32 + lane], L.bz.x); SA::add(accs[9 * 32 + lane], L.bx.y);
-    SA::add(accs[10 * 32 + lane], L.by.y); SA::add(accs[11 * 32 + lane], L.bz.y);
-    L.ax = L.ay = L.az = L.bx = L.by = L.bz = make_float2(0.f, 0.f);
+    nc -= sreg_region<SOFT, MASSES, NC, true, SPL>(stage, cap - nc, nc, j, J, owner, fin, L, a, eps2v, negu0v);
+    // sink k = 2 p + half of the lane keeps its three partials at accs[(3 k + d) * 32 + lane]
+#pragma unroll
+    for (int p = 0; p < SPL / 2; ++p) {
+        SA::add(accs[(6 * p + 0) * 32 + lane], L.ax[p].x); SA::add(accs[(6 * p + 1) * 32 + lane], L.ay[p].x);
+        SA::add(accs[(6 * p + 2) * 32 + lane], L.az[p].x); SA::add(accs[(6 * p + 3) * 32 + lane], L.ax[p].y);
+        SA::add(accs[(6 * p + 4) * 32 + lane], L.ay[p].y); SA::add(accs[(6 * p + 5) * 32 + lane], L.az[p].y);
+        L.ax[p] = L.ay[p] = L.az[p] = make_float2(0.f, 0.f);
+    }
     __syncwarp();
 }
 
-template <int SOFT, bool MASSES, int ACC, int NC>
-__global__ void __launch_bounds__(128, P2P_SREG_MINBLOCKS)
+template <int SOFT, bool MASSES, int ACC, int NC, int SPL>
+__global__ void __launch_bounds__(128, SPL == 4 ? P2P_SREG_MINBLOCKS : 3)
 pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
     extern __shared__ float4 smem_f4[];
     using SA = SregAcc<ACC>;
     using AT = typename SA::T;
     const int lane = threadIdx.x & 31;
-    unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_f4) + (threadIdx.x >> 5) * sreg_warp_bytes(cap);
+    unsigned char *wbase = reinterpret_cast<unsigned char *>(smem_f4) + (threadIdx.x >> 5) * sreg_warp_bytes(cap, SPL);
     float4 *stage = reinterpret_cast<float4 *>(wbase);
     AT *accs = reinterpret_cast<AT *>(wbase + (size_t)cap * 32);
-    SregCtx *ctx = reinterpret_cast<SregCtx *>(wbase + (size_t)cap * 32 + kSregAccBytes);
+    SregCtx *ctx = reinterpret_cast<SregCtx *>(wbase + (size_t)cap * 32 + sreg_acc_bytes(SPL));
     const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
     const unsigned lanes_below = (1u << lane) - 1u;
     unsigned long long evaluated = 0;  // pair interactions of staged sources with real sinks
@@ -250,25 +255,25 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
         }
         for (int s0 = 0; s0 < npart; s0 += 32) {
             const int ns = min(32, npart - s0);
-            const int G = (ns + 3) >> 2;
+            const int G = (ns + SPL - 1) / SPL;
             const int J = 32 / G;
             const int g = lane % G, jl = lane / G;
             const bool owner = jl < J;
             const int j = owner ? jl : 0;  // lanes past G * J shadow phase 0; their sums are never read
             const int first = ipart + s0;
-            SregLane L;
+            SregLane<SPL> L;
             {
-                L.sfirst = first + min(4 * g, ns - 1);
+                L.sfirst = first + min(SPL * g, ns - 1);
                 L.slast = first + ns - 1;
-                const float4 q0 = a.pos4[L.sfirst], q1 = a.pos4[min(L.sfirst + 1, L.slast)],
-                             q2 = a.pos4[min(L.sfirst + 2, L.slast)], q3 = a.pos4[min(L.sfirst + 3, L.slast)];
-                L.pax = make_float2(-q0.x, -q1.x);
-                L.pay = make_float2(-q0.y, -q1.y);
-                L.paz = make_float2(-q0.z, -q1.z);
-                L.pbx = make_float2(-q2.x, -q3.x);
-                L.pby = make_float2(-q2.y, -q3.y);
-                L.pbz = make_float2(-q2.z, -q3.z);
-                L.ax = L.ay = L.az = L.bx = L.by = L.bz = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int p = 0; p < SPL / 2; ++p) {
+                    const float4 q0 = a.pos4[min(L.sfirst + 2 * p, L.slast)];
+                    const float4 q1 = a.pos4[min(L.sfirst + 2 * p + 1, L.slast)];
+                    L.px[p] = make_float2(-q0.x, -q1.x);
+                    L.py[p] = make_float2(-q0.y, -q1.y);
+                    L.pz[p] = make_float2(-q0.z, -q1.z);
+                    L.ax[p] = L.ay[p] = L.az[p] = make_float2(0.f, 0.f);
+                }
             }
             {   // bounding box of the slice's sinks (sink frame), for the source classes
                 const float4 q = a.pos4[first + min(lane, ns - 1)];
@@ -292,7 +297,7 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
                 }
             }
 #pragma unroll
-            for (int k = 0; k < 12; ++k) SA::zero(accs[k * 32 + lane]);
+            for (int k = 0; k < 3 * SPL; ++k) SA::zero(accs[k * 32 + lane]);
             int ni = 0, nc = 0;
             unsigned staged = 0;
             // The row's entries in batches of 32, each batch's sources in groups of
@@ -332,8 +337,8 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
                 // consume at the row's end, and before a group that might not fit
                 // (at most twice: the second consume empties the stage)
                 for (bool fin = end; end ? (ni + nc > 0) : (ni + nc > cap - 32 * kSregRounds); fin = true)
-                    sreg_consume<SOFT, MASSES, ACC, NC>(stage, accs, cap, ni, nc, fin, j, J, owner, L, a, eps2v,
-                                                        negu0v);
+                    sreg_consume<SOFT, MASSES, ACC, NC, SPL>(stage, accs, cap, ni, nc, fin, j, J, owner, L, a, eps2v,
+                                                             negu0v);
                 if (end) break;
                 {
                     // every round's source located and its load issued first
@@ -394,7 +399,7 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
             }
             __syncwarp();
             if (lane < ns) {
-                const int gg = lane >> 2, sl = lane & 3;
+                const int gg = lane / SPL, sl = lane % SPL;
                 typename SA::Sum sx = 0, sy = 0, sz = 0;
                 for (int jj = 0; jj < J; ++jj) {
                     const int l = gg + jj * G;
