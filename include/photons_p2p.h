@@ -263,6 +263,38 @@ int p2p_pm_timings(p2p_pm *pm, float ms[5]);
  * potential (nullable outputs, N^3 doubles each). */
 int p2p_pm_download(p2p_pm *pm, double *mass_mesh, double *potential);
 
+/* ---- Far field within the cutoff: P2M, M2M, M2L, L2L, L2P --------------
+ * The multipole part of PhotoNs' short-range FMM on the kd-tree of the P2P
+ * pass: p2m / walk_m2m (src/operator.c:14-199, src/fmm.c:975-979), the M2L
+ * dual-tree walk and m2l with the erfc-truncated kernel (walk_task_m2l +
+ * task_compute_m2l, src/fmm.c:812-957 and :1188-1217; m2l LONGSHORT,
+ * src/operator.c:331-475), walk_l2l (:477-606) and l2p on the leaves that
+ * hold a local particle (:203-262, src/gravity.c:427-428); octupole order,
+ * the reference's 20-coefficient layout. The tree is the walk's
+ * (p2p_walk_tree: device arrays, e.g. from p2p_dtree_walk_tree); d_pos
+ * (3*npart doubles, SoA, tree order) and the leaf ranges are the pass's.
+ * d_acc (3*npart doubles, SoA, device) receives the far-field acceleration
+ * of the particles of active leaves, 0 for the others. Equal masses.
+ * min_r2: M2L tasks whose centres lie closer than sqrt(min_r2) contribute
+ * nothing. The reference's m2l tests abs(r2) <= 1e-15 with the integer abs()
+ * (src/operator.c:340-344), which skips every task with r2 < 1 in its length
+ * unit: min_r2 = 1 reproduces it, 1e-15 what the test evidently means.
+ * Queued on the session's stream; the M2L walk reads one count per tree
+ * level back to the host, so the call returns when the pass is done. */
+typedef struct p2p_fmm p2p_fmm;
+int p2p_fmm_create(p2p_session *s, p2p_fmm **out);
+int p2p_fmm_destroy(p2p_fmm *f);
+int p2p_fmm_far(p2p_fmm *f, const p2p_walk_tree *t, int npart, const double *d_pos, const int *d_leaf_ipart,
+                const int *d_leaf_npart, double mass, double split_radius, double cutoff, double open_angle,
+                double min_r2, double *d_acc);
+/* Counts and device times (ms: upward, walk, M2L, downward, total; nullable
+ * outputs) of the last p2p_fmm_far: M2L tasks, tasks applied (r2 >= min_r2),
+ * walk levels. */
+int p2p_fmm_stats(p2p_fmm *f, int64_t *n_m2l, int64_t *n_applied, int *levels, float ms[5]);
+/* Host copies (nullable) of the leaves' multipoles after P2M and their locals
+ * after L2L, 20 doubles per leaf in the reference's coefficient order. */
+int p2p_fmm_download(p2p_fmm *f, double *leaf_M, double *leaf_L);
+
 /* Host copy of the CSR rows of the last submitted chunk or walk (row_off:
  * nleaf+1 entries; row_src (nullable: rows not copied): row_off[nleaf]
  * entries). Call after p2p_pass_end. */

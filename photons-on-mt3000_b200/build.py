@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_SOURCES = ["p2p_core.cu", "p2p_noalloc.cu", "p2p_pair_sink_lanes.cu", "p2p_pair_source_lanes.cu",
                 "p2p_pair_source_lanes_x2.cu", "p2p_pair_source_lanes_x2_kahan.cu",
                 "p2p_pair_source_lanes_x2_f32.cu", "p2p_pair_plain.cu", "p2p_server.cu", "p2p_pair_sink_lanes_x2.cu",
-                "p2p_pair_sink_regs.cu", "p2p_tree.cu", "p2p_pm.cu"]
+                "p2p_pair_sink_regs.cu", "p2p_tree.cu", "p2p_pm.cu", "p2p_fmm.cu"]
 CUDA_HEADERS = ["p2p_kernels.cuh", "p2p_pass_kernels.cuh", "p2p_pair_kernels.cuh",
                 "p2p_device_common.cuh", "p2p_launch.h", "p2p_internal.h", "p2p_fit.h",
                 "p2p_pair_x2_impl.h", "p2p_csr.h", "p2p_args.h", "p2p_host_shared.h", "p2p_walk_kernels.cuh",

@@ -158,6 +158,12 @@ SIGNATURES = {
     "p2p_dtree_walk_tree": (_i, [_vp, ctypes.POINTER(WalkTree)]),
     "p2p_dtree_download": (_i, [_vp] + [_vp] * 11),
     "p2p_dtree_unpermute": (_i, [_vp, _vp, _vp, _vp]),
+    "p2p_fmm_create": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "p2p_fmm_destroy": (_i, [_vp]),
+    "p2p_fmm_far": (_i, [_vp, ctypes.POINTER(WalkTree), _i, _vp, _vp, _vp] + [_d] * 5 + [_vp]),
+    "p2p_fmm_stats": (_i, [_vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                           ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_float)]),
+    "p2p_fmm_download": (_i, [_vp, _vp, _vp]),
     "p2p_pm_create": (_i, [_vp, _i, _d, _d, ctypes.POINTER(_vp)]),
     "p2p_pm_destroy": (_i, [_vp]),
     "p2p_pm_forces": (_i, [_vp, _i, _vp, _vp, _d, _vp]),

@@ -220,6 +220,63 @@ class DeviceWalkTree:
                                    t[6].data_ptr())
 
 
+class FarField:
+    """The far field of the short-range force within the cutoff (p2p_fmm_*):
+    PhotoNs' P2M, M2M, M2L walk and M2L, L2L and L2P (src/operator.c,
+    src/fmm.c:812-957, :1188-1217) on the GPU, on the kd-tree of the pass."""
+
+    def __init__(self, session):
+        self.lib = session.lib
+        self.session = session
+        h = ctypes.c_void_p()
+        _check(self.lib, self.lib.p2p_fmm_create(session.h, ctypes.byref(h)))
+        self.h = h
+        self.nleaf = 0
+
+    def far(self, tree, d_pos, d_leaf_ipart, d_leaf_npart, npart, mass, split_radius, cutoff, open_angle,
+            min_r2, d_acc):
+        """tree: an abi.WalkTree of device arrays (DeviceTree.struct); the
+        other arrays are device pointers (ints); d_acc receives (3, npart)
+        far-field accelerations in tree order."""
+        self.nleaf = tree.nleaf
+        _check(self.lib, self.lib.p2p_fmm_far(self.h, ctypes.byref(tree), npart, d_pos, d_leaf_ipart, d_leaf_npart,
+                                              float(mass), float(split_radius), float(cutoff), float(open_angle),
+                                              float(min_r2), d_acc))
+
+    def stats(self):
+        """M2L tasks, tasks applied, walk levels and device ms (upward, walk,
+        m2l, downward, total) of the last far()."""
+        n, a, lv = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int()
+        ms = (ctypes.c_float * 5)()
+        _check(self.lib, self.lib.p2p_fmm_stats(self.h, ctypes.byref(n), ctypes.byref(a), ctypes.byref(lv), ms))
+        return dict(n_m2l=n.value, n_applied=a.value, levels=lv.value,
+                    ms=dict(zip(["upward", "walk", "m2l", "downward", "total"], list(ms))))
+
+    def download(self):
+        """(leaf multipoles, leaf locals), each (nleaf, 20)."""
+        m, l = np.empty((self.nleaf, 20)), np.empty((self.nleaf, 20))
+        _check(self.lib, self.lib.p2p_fmm_download(self.h, m.ctypes.data_as(ctypes.c_void_p),
+                                                   l.ctypes.data_as(ctypes.c_void_p)))
+        return m, l
+
+    def close(self):
+        if self.h:
+            self.lib.p2p_fmm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ParticleMesh:
     """The PM long-range force (p2p_pm_*): PhotoNs' partmesh_kick force part
     (src/partmesh.c:12-1470, src/conv.f90:239-330) for one periodic domain on

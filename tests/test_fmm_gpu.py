@@ -1,0 +1,84 @@
+"""The GPU far field (p2p_fmm_far, csrc/p2p_fmm.cu) against the reference's
+own (p2m, m2m, walk_task_m2l + m2l, walk_l2l, l2p from src/operator.c and
+src/fmm.c, compiled from the reference sources into oracle/_ref): the same
+kd-tree (built on the GPU, equal to the reference's node for node), the
+same M2L task count, the leaves' multipoles within 1e-12 and their final
+locals within 1e-10 of each coefficient's largest magnitude, and the
+far-field accelerations within 1e-10 of their rms. The reference sums in its
+own order (walk order per sink, its term order in each operator); these
+bounds cover the reassociation.
+
+Cases: the clustered mix in a box of 1000 (where the reference's m2l applies
+its tasks) at 64^3 and 128^3 with min_r2 = 1 (the reference's integer-abs
+test); the same particles in a unit box, where the reference drops every
+task and so does min_r2 = 1, while min_r2 = 1e-15 applies them all; the
+lattice drop-in settings, which make no M2L task."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from photons_p2p import workloads as W
+from photons_p2p.p2p import DeviceTree, FarField, Session
+
+from test_fmm import clustered, ref_fmm
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_available("libref_walk.so"),
+                                 reason="oracle/_ref walk harness not built")]
+
+
+def gpu_far(cfg, allpos, tag, mass, min_r2):
+    import torch
+
+    dev = torch.device("cuda", 0)
+    d_all = torch.from_numpy(np.ascontiguousarray(allpos)).to(dev)
+    d_tag = torch.from_numpy(np.ascontiguousarray(tag, dtype=np.int32)).to(dev)
+    torch.cuda.synchronize()
+    with Session(0) as s, DeviceTree(s, d_all, d_tag, cfg.maxleaf, cfg.box) as t, FarField(s) as ff:
+        d_pos, d_perm, d_ip, d_np = t.device_arrays()
+        acc = torch.empty((3, t.npart), dtype=torch.float64, device=dev)
+        ff.far(t.struct, d_pos, d_ip, d_np, t.npart, mass, cfg.split_radius, cfg.cutoff_radius, cfg.open_angle,
+               min_r2, acc.data_ptr())
+        st = ff.stats()
+        M, L = ff.download()
+        perm = t.download()["perm"]
+        return acc.cpu().numpy(), M, L, st, perm
+
+
+def scale_err(got, ref):
+    """Largest difference per coefficient over its largest magnitude."""
+    den = np.abs(ref).max(axis=0)
+    den[den == 0] = 1.0
+    return (np.abs(got - ref).max(axis=0) / den).max()
+
+
+@pytest.mark.parametrize("side", [64, 128])
+def test_matches_reference_box_1000(gpu, side):
+    cfg, allpos, tag, mass = clustered(side, 1000.0)
+    ref = ref_fmm(cfg, allpos, tag, mass)
+    acc, M, L, st, perm = gpu_far(cfg, allpos, tag, mass, 1.0)
+    assert np.array_equal(perm, ref["perm"])
+    assert st["n_m2l"] == ref["n_m2l"] > 0
+    assert 0 < st["n_applied"] <= st["n_m2l"]
+    assert scale_err(M, ref["leaf_M"]) <= 1e-12
+    assert scale_err(L, ref["leaf_L"]) <= 1e-10
+    rms = np.sqrt((ref["acc"] ** 2).sum(0).mean())
+    assert rms > 0 and np.abs(acc - ref["acc"]).max() <= 1e-10 * rms
+
+
+def test_unit_box(gpu):
+    cfg, allpos, tag, mass = clustered(64, 1.0)
+    ref = ref_fmm(cfg, allpos, tag, mass)
+    acc, M, L, st, _ = gpu_far(cfg, allpos, tag, mass, 1.0)
+    assert st["n_m2l"] == ref["n_m2l"] > 0 and st["n_applied"] == 0
+    assert not np.any(acc) and not np.any(ref["acc"])
+    acc2, _, _, st2, _ = gpu_far(cfg, allpos, tag, mass, 1e-15)
+    assert st2["n_applied"] == st2["n_m2l"] and np.abs(acc2).max() > 0
+
+
+def test_lattice_no_m2l(gpu):
+    cfg = W.ref_dropin_config(32, 64, 32)
+    pos = W.lattice_gaussian(32, 0.2, W.rng(1))
+    allpos, tag = W.with_ghosts(pos, cfg)
+    acc, M, L, st, _ = gpu_far(cfg, allpos, tag, 1.0 / pos.shape[1], 1.0)
+    assert st["n_m2l"] == 0 and not np.any(acc) and not np.any(L)
