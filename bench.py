@@ -1,7 +1,7 @@
 """Benchmark of the B200 P2P short-range force pass.
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                [--workload c2|c1|c2_128|c4|pm] [--form split|plain]
+                [--workload c2|c1|c2_128|c4|pm|fmm] [--form split|plain]
 
 A step is one force pass over the workload's interaction lists. The default
 workload is the 256^3 clustered configuration (60% uniform, 40% in 2,000 NFW
@@ -34,6 +34,9 @@ from the caller-side tree build + walk (the reference's src/fmm.c algorithm).
 --workload c4 runs the serving configuration alone: 512 boxes, Poisson
 arrivals at 0.25, 0.5, 1, 2 and 4 times the measured saturation rate.
 --workload pm runs the PM leg alone (256^3 clustered particles, mesh 256^3).
+--workload fmm runs the far field within the cutoff (P2M, M2M, M2L, L2L,
+L2P) on the clustered particles with open angle 0.4, beside the reference's
+own M2L timed on one host core.
 
 With --gpus N > 1 (torchrun, one rank per GPU) every rank runs its own
 independent box (replicas, no collective on the data path); the timed
@@ -346,6 +349,86 @@ def pm_leg(sess, cfg, raw_pos, dev, hbm_peak, cpu=True, steps=5, warmup=3):
         gpu1 = timed(pm, p1, steps, warmup)
     out["lattice_32^3_mesh_64^3"] = {"gpu_ms": gpu1["total"], "cpu_oracle_ms": cpu_ms,
                                      "cpu_oracle": "numpy, 1 thread (the reference's PM needs MPI and 2DECOMP&FFT)"}
+    return out
+
+
+def _stdout_closed(fn):
+    """fn() with the process's stdout closed (the reference's m2l prints a
+    line for every task it skips)."""
+    fd = os.dup(1)
+    nul = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(nul, 1)
+    try:
+        return fn()
+    finally:
+        os.dup2(fd, 1)
+        os.close(fd)
+        os.close(nul)
+
+
+def run_fmm(args, local):
+    """The far field within the cutoff (p2p_fmm_far) on the clustered
+    particles with the reference's open angle 0.4: at 256^3 in the unit box
+    with every M2L task applied (min_r2 = 1e-15), and at 128^3 in a box of
+    1000, where the reference's own FMM applies its tasks (min_r2 = 1, its
+    integer-abs test), beside the reference's task_compute_m2l and l2p timed
+    on one host core (its own dtime_m2l timer)."""
+    import torch
+
+    from photons_p2p.p2p import DeviceTree, FarField, Session
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    warm = max(3, args.warmup)
+
+    def gpu(cfg, allpos, tag, mass, min_r2):
+        d_all = torch.from_numpy(np.ascontiguousarray(allpos)).to(dev)
+        d_tag = torch.from_numpy(np.ascontiguousarray(tag, dtype=np.int32)).to(dev)
+        torch.cuda.synchronize()
+        with Session(local) as s, DeviceTree(s, d_all, d_tag, cfg.maxleaf, cfg.box) as t, FarField(s) as ff:
+            d_pos, _, d_ip, d_np = t.device_arrays()
+            acc = torch.empty((3, t.npart), dtype=torch.float64, device=dev)
+            rows, wall = [], []
+            for k in range(warm + args.steps):
+                a = time.perf_counter()
+                ff.far(t.struct, d_pos, d_ip, d_np, t.npart, mass, cfg.split_radius, cfg.cutoff_radius,
+                       cfg.open_angle, min_r2, acc.data_ptr())
+                el = time.perf_counter() - a
+                st = ff.stats()
+                if k >= warm:
+                    rows.append(st["ms"])
+                    wall.append(el)
+            ms = {key: float(np.mean([r[key] for r in rows])) for key in rows[0]}
+            return {"particles_with_ghosts": int(t.npart), "leaves": int(t.nleaf), "nodes": int(t.nnode),
+                    "m2l_tasks": st["n_m2l"], "m2l_applied": st["n_applied"], "walk_levels": st["levels"],
+                    "device_ms": ms, "wall_ms": 1e3 * float(np.mean(wall)),
+                    "m2l_tasks_per_s": st["n_m2l"] / (ms["m2l"] * 1e-3) if ms["m2l"] > 0 else None}
+
+    cfg = W.scaled(W.c2_config(), open_angle=0.4)
+    pos = W.c2_positions()
+    allpos, tag = W.with_ghosts(pos, cfg)
+    out = {"workload": "fmm_clustered_256^3_open_0.4", "steps": args.steps, "warmup": warm,
+           "unit_box_256": gpu(cfg, allpos, tag, 1.0 / pos.shape[1], 1e-15)}
+    del allpos, tag, pos
+    cfgb = W.scaled(W.c2_config(), n_side=128, mesh=128, eps=1000.0 / (40 * 128), open_angle=0.4, box=1000.0)
+    posb = W.c2_positions(128) * 1000.0
+    allb, tagb = W.with_ghosts(posb, cfgb)
+    massb = 1.0 / posb.shape[1]
+    out["box_1000_128"] = g = gpu(cfgb, allb, tagb, massb, 1.0)
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        if O.ref_available("libref_walk.so"):
+            r = _stdout_closed(lambda: O.RefWalk("libref_walk.so").fmm(
+                allb, tagb, cfgb.maxleaf, cfgb.box, cfgb.split_radius, cfgb.cutoff_radius, cfgb.eps, massb,
+                cfgb.open_angle))
+            out["cpu_baseline"] = {"kind": "reference", "cores": 1, "sample": "the 128^3 box-1000 case, whole",
+                                   "m2l_s": r["m2l_s"], "l2p_s": r["l2p_s"], "m2l_tasks": r["n_m2l"],
+                                   "m2l_tasks_per_s": r["n_m2l"] / r["m2l_s"] if r["m2l_s"] > 0 else None,
+                                   "gpu_m2l_speedup": (r["m2l_s"] * 1e3) / g["device_ms"]["m2l"]
+                                   if g["device_ms"]["m2l"] > 0 else None}
+        else:
+            out["cpu_baseline"] = {"unavailable": "oracle/_ref not built"}
     return out
 
 
@@ -958,6 +1041,14 @@ def main():
     if args.workload == "c3":
         if rank == 0:
             print(json.dumps(run_batching(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    if args.workload == "fmm":
+        if rank == 0:
+            print(json.dumps(run_fmm(args, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()

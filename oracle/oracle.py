@@ -186,10 +186,11 @@ class RefWalk:
         """The reference's far field (ref_harness_fmm): tree order and leaf
         table as run() gives them, the leaves' multipoles M and locals L
         (nleaf, 20), the far-field accelerations of l2p (3, n) in tree order,
-        and the counts of M2L tasks, m2l calls and nodes."""
+        the counts of M2L tasks, m2l calls and nodes, and the seconds of
+        the reference's task_compute_m2l (its own timer) and of the l2p."""
         f = self.L.ref_harness_fmm
         f.restype = ctypes.c_int
-        f.argtypes = ([ctypes.c_int, _vp, _vp, ctypes.c_int] + [ctypes.c_double] * 6 + [_vp] * 10)
+        f.argtypes = ([ctypes.c_int, _vp, _vp, ctypes.c_int] + [ctypes.c_double] * 6 + [_vp] * 11)
         pos = np.ascontiguousarray(pos, np.float64)
         tag = np.ascontiguousarray(tag, np.int32)
         n = pos.shape[1]
@@ -203,14 +204,16 @@ class RefWalk:
         ll = np.empty((n + 1, 20))
         acc = np.empty((3, n))
         counts = np.zeros(3, np.int64)
+        times = np.zeros(2)
         nl = f(n, _p(pos), _p(tag), maxleaf, boxsize, split_radius, cutoff_radius, soften, mass, open_angle,
-               _p(perm), _p(ip), _p(npt), _p(ctr), _p(wid), _p(act), _p(lm), _p(ll), _p(acc), _p(counts))
+               _p(perm), _p(ip), _p(npt), _p(ctr), _p(wid), _p(act), _p(lm), _p(ll), _p(acc), _p(counts), _p(times))
         if nl < 0:
             raise RuntimeError("reference harness failed")
         return dict(perm=perm, leaf_ipart=ip[:nl].copy(), leaf_npart=npt[:nl].copy(),
                     leaf_active=act[:nl].copy(), leaf_center=ctr[:nl].copy(), leaf_width=wid[:nl].copy(),
                     leaf_M=lm[:nl].copy(), leaf_L=ll[:nl].copy(), acc=acc, n_m2l=int(counts[0]),
-                    n_m2l_calls=int(counts[1]), n_node=int(counts[2]))
+                    n_m2l_calls=int(counts[1]), n_node=int(counts[2]), m2l_s=float(times[0]),
+                    l2p_s=float(times[1]))
 
     def run(self, pos, tag, maxleaf, boxsize, split_radius, cutoff_radius, soften, mass,
             open_angle, len_task, collect_acc=False):

@@ -179,12 +179,15 @@ int ref_harness_run(int npart, const double *pos, const int *tag, int maxleaf,
  *                    walk_l2l (the M2L sums plus the parents' shifted locals)
  *   acc_out          SoA far-field accelerations of the l2p
  *   counts           [0] M2L tasks (idxM2L), [1] m2l calls, [2] nodes
+ *   times            [0] seconds of task_compute_m2l (the reference's own
+ *                    dtime_m2l), [1] seconds of the l2p loop
  * Returns the number of leaves, or -1.
  */
 int ref_harness_fmm(int npart, const double *pos, const int *tag, int maxleaf, double boxsize,
                     double split_radius, double cutoff_radius, double soften, double mass, double open_angle_in,
                     int *perm, int *leaf_ipart, int *leaf_npart, double *leaf_center, double *leaf_width,
-                    int *leaf_active, double *leaf_M, double *leaf_L, double *acc_out, long long *counts) {
+                    int *leaf_active, double *leaf_M, double *leaf_L, double *acc_out, long long *counts,
+                    double *times) {
     cpuType boxL[3], boxH[3];
     if (harness_setup(npart, pos, tag, maxleaf, boxsize, split_radius, cutoff_radius, soften, mass,
                       open_angle_in, 1 << 24, 1, boxL, boxH))
@@ -199,8 +202,11 @@ int ref_harness_fmm(int npart, const double *pos, const int *tag, int maxleaf, d
     restate_p2ppack_cln();
     for (int d = 0; d < 3; ++d)
         for (int n = 0; n < npart; ++n) acc[d][n] = 0.0;
+    const double t_l2p = dtime();
     for (int n = first_leaf; n < last_leaf; ++n)
         if (leaf[n].active >= 0) l2p(n);
+    times[0] = dtime_m2l;  /* the reference's own timer of task_compute_m2l (src/fmm.c:1188-1217) */
+    times[1] = dtime() - t_l2p;
     for (int l = 0; l < nleaf; ++l)
         for (int k = 0; k < NMULTI; ++k) leaf_L[(size_t)NMULTI * l + k] = leaf[first_leaf + l].L[k];
     counts[0] = idxM2L;

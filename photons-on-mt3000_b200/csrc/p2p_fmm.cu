@@ -12,9 +12,9 @@
 //              of :409-479) expanded breadth first on the GPU, a level of
 //              pending pairs per launch: a pair is accepted as an M2L task,
 //              opened into its child pairs, or dropped
-//   M2L        each sink (leaf or node) sums, over its tasks in increasing
-//              source order, the source multipole's contribution to its
-//              local expansion with the erfc-truncated kernel's derivatives
+//   M2L        each sink (leaf or node), one warp, sums over its tasks in
+//              increasing source order the source multipole's contribution
+//              to its local expansion with the erfc-truncated kernel's derivatives
 //              (m2l with LONGSHORT, src/operator.c:331-475)
 //   l2l + l2p  each leaf takes its ancestors' locals down its path from the
 //              root (l2l / walk_l2l, :477-606) and, if it holds a local
@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -334,52 +335,103 @@ __global__ void fmm_task_fill_kernel(WalkArgs w, const int2 *__restrict__ tasks,
     }
 }
 
-// M2L: sink s sums its tasks' contributions in increasing source order.
-__global__ void fmm_m2l_kernel(FmmArgs f, const int64_t *__restrict__ off, int *seg,
-                               unsigned long long *applied) {
+// M2L: one warp per sink. The sink's source codes are put in increasing
+// order (a bitonic sort in shared memory up to kM2LSort codes; above that a
+// rank sort from seg into seg2), lane j takes the sorted tasks j, j + 32, ...
+// and the lanes' partial locals are summed by a fixed shuffle tree: the same
+// order on every run, whatever order the walk emitted the tasks in.
+constexpr int kM2LWarps = 4;
+constexpr int kM2LSort = 2048;
+
+__global__ void __launch_bounds__(32 * kM2LWarps)
+fmm_m2l_kernel(FmmArgs f, const int64_t *__restrict__ off, const int *__restrict__ seg, int *__restrict__ seg2,
+               unsigned long long *applied) {
+    __shared__ int sbuf[kM2LWarps][kM2LSort];
     const WalkArgs &w = f.w;
+    const int lane = threadIdx.x & 31;
+    int *buf = sbuf[threadIdx.x >> 5];
     const int nsink = w.nleaf + w.nnode;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsink; s += gridDim.x * blockDim.x) {
-        const int64_t a = off[s], b = off[s + 1];
-        for (int64_t i = a + 1; i < b; ++i) {  // insertion sort of the sink's source codes
-            const int v = seg[i];
-            int64_t j = i - 1;
-            while (j >= a && seg[j] > v) {
-                seg[j + 1] = seg[j];
-                --j;
+    const int nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nsink; s += nwarp) {
+        const int64_t a = off[s], e = off[s + 1];
+        if (a < 0 || e < a || e > off[nsink]) {  // offsets out of order: record it, skip the sink
+            if (lane == 0) atomicOr(f.status, ST_WALK_ROW);
+            continue;
+        }
+        const int k = (int)(e - a);
+        const int *src = buf;
+        if (k <= kM2LSort) {
+            int p = 1;
+            while (p < k) p <<= 1;
+            for (int i = lane; i < p; i += 32) buf[i] = i < k ? seg[a + i] : INT_MAX;
+            __syncwarp();
+            for (int size = 2; size <= p; size <<= 1) {
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    for (int i = lane; i < p; i += 32) {
+                        const int j = i ^ stride;
+                        if (j > i) {
+                            const int x = buf[i], y = buf[j];
+                            if ((x > y) == ((i & size) == 0)) {
+                                buf[i] = y;
+                                buf[j] = x;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
             }
-            seg[j + 1] = v;
+        } else {
+            for (int i = lane; i < k; i += 32) {
+                const int v = seg[a + i];
+                int r = 0;
+                for (int j = 0; j < k; ++j) {
+                    const int x = seg[a + j];
+                    r += (x < v) || (x == v && j < i);
+                }
+                seg2[a + r] = v;
+            }
+            __syncwarp();
+            src = seg2 + a;
         }
         double L[kNC];
 #pragma unroll
-        for (int k = 0; k < kNC; ++k) L[k] = 0.0;
+        for (int c = 0; c < kNC; ++c) L[c] = 0.0;
         const int code = s < w.nleaf ? 2 * s : 2 * (s - w.nleaf) + 1;
         const double *cs = box_center(w, code);
-        unsigned long long used = 0;
-        for (int64_t t = a; t < b; ++t) {
-            const int src = seg[t];
-            const double *cb = box_center(w, src);
+        unsigned used = 0;
+        for (int t = lane; t < k; t += 32) {
+            const int sc = src[t];
+            const double *cb = box_center(w, sc);
             const double x = cs[0] - cb[0], y = cs[1] - cb[1], z = cs[2] - cb[2];
             const double r2 = x * x + y * y + z * z;
             if (!(r2 >= f.min_r2)) continue;
             ++used;
-            const double *Msrc = (src & 1) ? f.nodeM + (size_t)kNC * (src >> 1) : f.leafM + (size_t)kNC * (src >> 1);
+            const double *Msrc = (sc & 1) ? f.nodeM + (size_t)kNC * (sc >> 1) : f.leafM + (size_t)kNC * (sc >> 1);
             double m[kNC], D[kNC];
 #pragma unroll
-            for (int k = 0; k < kNC; ++k) m[k] = Msrc[k];
+            for (int c = 0; c < kNC; ++c) m[c] = Msrc[c];
             kernel_derivs(x, y, z, r2, f.irs, D);
 #pragma unroll
-            for (int k = 0; k < kNC; ++k) {
+            for (int c = 0; c < kNC; ++c) {
                 double acc = 0.0;
 #pragma unroll
                 for (int j = 0; j < kNC; ++j)
-                    if (sum_idx(k, j) >= 0) acc += m[j] * D[sum_idx(k, j)];
-                L[k] += acc;
+                    if (sum_idx(c, j) >= 0) acc += m[j] * D[sum_idx(c, j)];
+                L[c] += acc;
             }
         }
 #pragma unroll
-        for (int k = 0; k < kNC; ++k) f.sinkL[(size_t)kNC * s + k] = L[k];
-        if (used) atomicAdd(applied, used);
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int c = 0; c < kNC; ++c) L[c] += __shfl_down_sync(kFull, L[c], o);
+            used += __shfl_down_sync(kFull, used, o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < kNC; ++c) f.sinkL[(size_t)kNC * s + c] = L[c];
+            if (used) atomicAdd(applied, (unsigned long long)used);
+        }
+        __syncwarp();  // the shared buffer is rewritten by the next sink
     }
 }
 
@@ -482,7 +534,7 @@ int blocks_for(long long n, int threads) {
 struct p2p_fmm {
     int device = 0;
     cudaStream_t stream = nullptr;
-    DevBufF parents, leafM, nodeM, sinkL, leafL, front[2], tasks, counts, off, tiles, seg, ctrl;
+    DevBufF parents, leafM, nodeM, sinkL, leafL, front[2], tasks, counts, off, tiles, seg, seg2, ctrl;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     long long n_m2l = 0, n_applied = 0;
     int levels = 0, nleaf = 0, nnode = 0;
@@ -522,7 +574,7 @@ P2P_API int p2p_fmm_destroy(p2p_fmm *f) {
     cudaSetDevice(f->device);
     cudaStreamSynchronize(f->stream);
     DevBufF *bufs[] = {&f->parents, &f->leafM, &f->nodeM, &f->sinkL, &f->leafL, &f->front[0], &f->front[1],
-                       &f->tasks, &f->counts, &f->off, &f->tiles, &f->seg, &f->ctrl};
+                       &f->tasks, &f->counts, &f->off, &f->tiles, &f->seg, &f->seg2, &f->ctrl};
     for (DevBufF *b : bufs)
         if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : f->ev)
@@ -665,6 +717,7 @@ P2P_API int p2p_fmm_far(p2p_fmm *f, const p2p_walk_tree *t, int npart, const dou
     int *count = (int *)f->counts.p, *fill = count + nsink;
     int64_t *off = (int64_t *)f->off.p;
     FMM_TRY(grow(f->seg, sizeof(int) * (size_t)std::max<long long>(ntask, 1)));
+    FMM_TRY(grow(f->seg2, sizeof(int) * (size_t)std::max<long long>(ntask, 1)));
     FMM_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * 2 * (size_t)nsink, st), "FMM m2l");
     if (ntask)
         fmm_task_count_kernel<<<blocks_for(ntask, threads), threads, 0, st>>>(a.w, (const int2 *)f->tasks.p, ntask,
@@ -673,11 +726,13 @@ P2P_API int p2p_fmm_far(p2p_fmm *f, const p2p_walk_tree *t, int npart, const dou
     int64_t *tiles = (int64_t *)f->tiles.p;
     scan_tiles_kernel<<<ntiles, kScanThreads, 0, st>>>(count, nsink, off, tiles);
     scan_sums_kernel<<<1, kScanThreads, 0, st>>>(tiles, ntiles, off + nsink);
-    scan_add_kernel<<<blocks_for(nsink, threads), threads, 0, st>>>(off, nsink, tiles);
+    // one thread per element (the kernel has no grid-stride loop)
+    scan_add_kernel<<<(nsink + threads - 1) / threads, threads, 0, st>>>(off, nsink, tiles);
     if (ntask)
         fmm_task_fill_kernel<<<blocks_for(ntask, threads), threads, 0, st>>>(a.w, (const int2 *)f->tasks.p, ntask,
                                                                               off, fill, (int *)f->seg.p);
-    fmm_m2l_kernel<<<blocks_for(nsink, 128), 128, 0, st>>>(a, off, (int *)f->seg.p, ctrl + 2);
+    fmm_m2l_kernel<<<(int)std::min<long long>(((long long)nsink + kM2LWarps - 1) / kM2LWarps, 148LL * 16),
+                     32 * kM2LWarps, 0, st>>>(a, off, (const int *)f->seg.p, (int *)f->seg2.p, ctrl + 2);
     FMM_CUDA(cudaEventRecord(f->ev[3], st), "FMM m2l");
     fmm_downward_kernel<<<blocks_for(nleaf, 128), 128, 0, st>>>(a, d_acc);
     FMM_CUDA(cudaEventRecord(f->ev[4], st), "FMM downward");
@@ -688,6 +743,7 @@ P2P_API int p2p_fmm_far(p2p_fmm *f, const p2p_walk_tree *t, int npart, const dou
     f->n_applied = (long long)h2[0];
     count_launches(4 + f->levels + (ntask ? 5 : 3));
     if ((int)h2[1] & ST_WALK_TREE) return report_error(P2P_ERR_ARG, "FMM: a child code outside the tree");
+    if ((int)h2[1] & ST_WALK_ROW) return report_error(P2P_ERR_STATE, "FMM: M2L task offsets out of order");
     return P2P_OK;
 }
 
