@@ -539,7 +539,8 @@ def run_ours(args, rank, world, dist):
 
         prm, rec = autotune.tune(cfg, tl, form, mass, device=local, sample_pairs=args.tune_pairs,
                                  cache_path=args.tune_cache)
-        tuned = {k: rec[k] for k in ("key", "variant", "stage", "warps", "sample_pairs", "cached")}
+        tuned = {k: rec.get(k, 1) for k in ("key", "variant", "stage", "warps", "leaf_warps", "sample_pairs",
+                                             "cached")}
     with Session(local) as sess:
         fp32_peak = sess.measure_fp32_peak()
         fp64_peak = sess.measure_fp64_peak()
@@ -870,7 +871,7 @@ def run_batching(args, local):
         r = {"leaf_cap": cap, "leaves": int(nleaf), "leaf_npart_q0_25_50_75_100": qs,
              "mean_leaf": mean_leaf, "rows": int(rows), "rows_per_sink_leaf": rows / max(1, nleaf),
              "chunks": len(chunks), "pairs": int(pairs), "pass_s": pass_s, "pairs_per_s": pairs / pass_s,
-             "tuned": {k: rec[k] for k in ("key", "variant", "stage", "warps", "cached")},
+             "tuned": {k: rec.get(k, 1) for k in ("key", "variant", "stage", "warps", "leaf_warps", "cached")},
              "lists_host_s": round(lists_s, 1)}
         log(f"[batching] cap {cap}: pass {pass_s:.3f} s  {pairs / pass_s:.3e} pairs/s  shape "
             f"{rec['variant']}/{rec['stage']}/{rec['warps']}")

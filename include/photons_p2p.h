@@ -71,6 +71,11 @@ typedef struct {
     double poly_tol;     /* FP32 forms: bound on x * |dH| of the fitted polynomial
                             (H: g(x) = 1 - x^3 H(x^2)); the smallest degree meeting it
                             is used; 0 = default 1e-7 (degree 10 at x_cut 2.25) */
+    int warps_per_leaf;  /* sink-register mappings: 1, 2 or 4 warps share one sink leaf's
+                            row, each taking a contiguous share of its list entries and
+                            adding its partial forces with FP64 atomics (the summation
+                            order then varies between runs); 0 = 1. Ignored by the
+                            other mappings */
 } p2p_params;
 
 /* Lane mappings of the FP32 pair kernel. */
@@ -88,6 +93,9 @@ typedef struct {
                                              pairs) and takes every J-th staged source; sources
                                              are classified per particle against the sink slice's
                                              box (dropped / no cutoff test / cutoff test) */
+#define P2P_VARIANT_SINK_REGS8 7          /* the same with eight sinks per lane (four packed pairs)
+                                             and 64-sink slices: a leaf of up to 64 particles
+                                             stages each source once */
 
 typedef struct p2p_session p2p_session;
 

@@ -38,6 +38,7 @@ inline void fill_pass_scalars(PairArgs &a, const p2p_params &p, const PolyFit &f
     a.coeff = 2.0 * (1.0 / std::sqrt(M_PI));
     a.xcut = p.x_cut;
     a.mass_eq = p.mass;
+    a.leaf_warps = p.warps_per_leaf > 1 ? p.warps_per_leaf : 1;
 }
 
 }  // namespace p2p

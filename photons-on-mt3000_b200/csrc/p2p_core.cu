@@ -159,7 +159,9 @@ int validate_params(const p2p_params *p) {
         return fail(P2P_ERR_ARG, "stage_sources must be a multiple of 32 in [0, 1024]");
     if (p->blocks_per_sm < 0 || p->blocks_per_sm > 32)
         return fail(P2P_ERR_ARG, "blocks_per_sm must be in [0, 32]");
-    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SINK_REGS)
+    if (p->warps_per_leaf != 0 && p->warps_per_leaf != 1 && p->warps_per_leaf != 2 && p->warps_per_leaf != 4)
+        return fail(P2P_ERR_ARG, "warps_per_leaf must be 0, 1, 2 or 4");
+    if (p->kernel_variant < P2P_VARIANT_AUTO || p->kernel_variant > P2P_VARIANT_SINK_REGS8)
         return fail(P2P_ERR_ARG, "unknown kernel_variant %d", p->kernel_variant);
     if (p->form != P2P_FORM_PLAIN_FP64 && p->kernel_variant != P2P_VARIANT_SINK_LANES &&
         p->warps_per_block > 4)
@@ -170,7 +172,7 @@ int validate_params(const p2p_params *p) {
         const size_t smem = p->form == P2P_FORM_PLAIN_FP64 ? pair_smem_plain(w, st)
                             : std::max(std::max(std::max(pair_smem_x2(w, st), pair_smem_sx2(w, st)),
                                                 pair_smem_split(w, st, true)),
-                                       pair_smem_sreg(w, st));
+                                       pair_smem_sreg(w, st, 8));
         if (smem > (size_t)227 * 1024)
             return fail(P2P_ERR_ARG, "warps_per_block * stage_sources needs %zu B of shared memory (> 227 KB)", smem);
     }
@@ -196,7 +198,8 @@ bool packed_lanes(const p2p_params &p) {
 // sink-register kernel, which also drops single source particles).
 bool sink_regs(const p2p_params &p) {
     return is_fp32_form(p.form) &&
-           (p.kernel_variant == P2P_VARIANT_SINK_REGS || p.kernel_variant == P2P_VARIANT_AUTO);
+           (p.kernel_variant == P2P_VARIANT_SINK_REGS || p.kernel_variant == P2P_VARIANT_SINK_REGS8 ||
+            p.kernel_variant == P2P_VARIANT_AUTO);
 }
 bool counts_evaluated(const p2p_params &p) { return sink_regs(p); }
 
@@ -220,6 +223,7 @@ int launch_pair(p2p_session *s, const PairArgs &a) {
     L.dry_run = s->dry_run;
     L.occ = &s->occupancy;
     L.sink_pairs = p.kernel_variant == P2P_VARIANT_SOURCE_LANES_X2_S16 ? 8 : 16;
+    L.sreg_spl = p.kernel_variant == P2P_VARIANT_SINK_REGS8 ? 8 : 4;
     PairLaunchResult r;
     if (p.form == P2P_FORM_PLAIN_FP64)
         r = launch_pair_plain(L, a);

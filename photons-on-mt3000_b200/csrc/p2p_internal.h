@@ -78,6 +78,7 @@ struct PairArgs {
     // [seg_item[k], seg_item[k + 1]) are the sink leaves seg_leaf[k] + 0, 1, ...
     // of box k; nleaf then counts the items. nseg = 0: item i is leaf i.
     int nseg;
+    int leaf_warps;          // sink-register kernels: warps sharing one sink leaf's row (<= 1: one)
     int seg_item[kMaxSeg + 1];
     int seg_leaf[kMaxSeg];
 };

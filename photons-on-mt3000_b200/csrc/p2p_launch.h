@@ -28,6 +28,7 @@ struct PairLaunch {
     OccupancyCache *occ;
     int max_blocks = 0; // > 0: cap on the persistent grid (a share of the GPU)
     int sink_pairs = 16; // packed source-lane kernel: sink pairs per slice (16 or 8)
+    int sreg_spl = 4;    // sink-register kernel: sinks per lane (4: 32-sink slices, 8: 64)
 };
 
 struct PairLaunchResult {
@@ -49,11 +50,8 @@ inline size_t pair_smem_sx2(int warps, int stage) { return (size_t)warps * (stag
 // accumulators + staging context; its stage holds at least kSregMinStage sources (one staging group)
 constexpr int kSregMinStage = 128;
 inline int sreg_stage(int stage) { return stage < kSregMinStage ? kSregMinStage : stage; }
-#ifndef P2P_SREG_SPL
-#define P2P_SREG_SPL 4  // sinks per lane of the sink-register kernel
-#endif
-inline size_t pair_smem_sreg(int warps, int stage) {
-    return (size_t)warps * ((size_t)sreg_stage(stage) * 32 + 3 * P2P_SREG_SPL * 32 * 8 + 1024);
+inline size_t pair_smem_sreg(int warps, int stage, int spl = 4) {
+    return (size_t)warps * ((size_t)sreg_stage(stage) * 32 + 3 * (size_t)spl * 32 * 8 + 1024);
 }
 
 // Persistent grid for `kernel`: blocks_per_sm, or as many as registers and

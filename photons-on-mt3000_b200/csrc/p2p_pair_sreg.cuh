@@ -1,9 +1,10 @@
 // Sink-register pair kernel of the FP32 forms (P2P_VARIANT_SINK_REGS).
 //
-// A slice of ns <= 32 sink particles of a sink leaf is split into G =
-// ceil(ns / SPL) groups of SPL sinks (SPL = P2P_SREG_SPL, 4; 8 was measured
-// slower: 168 registers, 3 blocks per SM, more padded sinks); lane (g, j) =
-// (lane % G, lane / G), j < J = floor(32 / G), keeps group g's sinks in
+// A slice of ns <= 8 SPL sink particles of a sink leaf (32 with SPL = 4,
+// P2P_VARIANT_SINK_REGS; 64 with SPL = 8, P2P_VARIANT_SINK_REGS8, whose
+// 168 registers leave 3 blocks per SM) is split into G = ceil(ns / SPL)
+// groups of SPL sinks; lane (g, j) = (lane % G, lane / G), j < J = floor(32 /
+// G), keeps group g's sinks in
 // registers as SPL / 2 packed sink pairs and takes the staged sources j,
 // j + J, j + 2J, ... of the row. A staged source is read as two 16-byte
 // shared-memory loads (stored pre-duplicated: (x, x, y, y), (z, z, w,
@@ -25,6 +26,10 @@
 // row's end runs whole iterations only (two sources for every lane) and
 // leaves the remainder of each region in place for the next one; the
 // per-lane guarded tail runs once, at the end of the slice.
+//
+// With PairArgs::leaf_warps = W > 1 a sink leaf is W work items, each a
+// contiguous share of the row's list entries, whose partial forces are added
+// with FP64 atomics (a long row is spread over W warps).
 //
 // Band pairs (FP32 u within the band around x_cut^2) are re-decided from FP64
 // positions by the lane that met them (band_pair), as in the other packed
@@ -234,13 +239,21 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
     const float2 eps2v = make_float2(a.eps2, a.eps2), negu0v = make_float2(-a.u0, -a.u0);
     const unsigned lanes_below = (1u << lane) - 1u;
     unsigned long long evaluated = 0;  // pair interactions of staged sources with real sinks
+    constexpr int SLICE = 8 * SPL;     // sinks of a slice: G <= 8 groups, J >= 4 phases
+    const int W = a.leaf_warps > 1 ? a.leaf_warps : 1;  // warps sharing a row (work items per leaf)
     for (;;) {
         int item = 0;
         if (lane == 0) item = atomicAdd(a.queue, 1);
         item = __shfl_sync(kFull, item, 0);
-        if (item >= a.nleaf) break;
-        const int li = item_leaf(a, item, lane);
-        const int64_t rb = a.row_off[li], re = a.row_off[li + 1];
+        if (item >= a.nleaf * W) break;
+        const int li = item_leaf(a, item / W, lane);
+        int64_t rb = a.row_off[li], re = a.row_off[li + 1];
+        if (W > 1) {  // this item's contiguous share of the row's entries
+            const int part = item % W;
+            const int64_t len = re - rb;
+            re = rb + len * (part + 1) / W;
+            rb = rb + len * part / W;
+        }
         if (rb >= re) continue;
         int ipart, npart;
         {
@@ -253,8 +266,8 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
                 ctx->mhx = mt.hx; ctx->mhy = mt.hy; ctx->mhz = mt.hz;
             }
         }
-        for (int s0 = 0; s0 < npart; s0 += 32) {
-            const int ns = min(32, npart - s0);
+        for (int s0 = 0; s0 < npart; s0 += SLICE) {
+            const int ns = min(SLICE, npart - s0);
             const int G = (ns + SPL - 1) / SPL;
             const int J = 32 / G;
             const int g = lane % G, jl = lane / G;
@@ -278,6 +291,11 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
             {   // bounding box of the slice's sinks (sink frame), for the source classes
                 const float4 q = a.pos4[first + min(lane, ns - 1)];
                 float lx = q.x, ly = q.y, lz = q.z, hx = q.x, hy = q.y, hz = q.z;
+                for (int sk = lane + 32; sk < ns; sk += 32) {
+                    const float4 r = a.pos4[first + sk];
+                    lx = fminf(lx, r.x); ly = fminf(ly, r.y); lz = fminf(lz, r.z);
+                    hx = fmaxf(hx, r.x); hy = fmaxf(hy, r.y); hz = fmaxf(hz, r.z);
+                }
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) {
                     lx = fminf(lx, __shfl_xor_sync(kFull, lx, off));
@@ -398,8 +416,8 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
                 done += 32 * kSregRounds;
             }
             __syncwarp();
-            if (lane < ns) {
-                const int gg = lane / SPL, sl = lane % SPL;
+            for (int sk = lane; sk < ns; sk += 32) {
+                const int gg = sk / SPL, sl = sk % SPL;
                 typename SA::Sum sx = 0, sy = 0, sz = 0;
                 for (int jj = 0; jj < J; ++jj) {
                     const int l = gg + jj * G;
@@ -407,10 +425,18 @@ pair_sreg_kernel(const __grid_constant__ PairArgs a, const int cap) {
                     sy += SA::value(accs[(sl * 3 + 1) * 32 + l]);
                     sz += SA::value(accs[(sl * 3 + 2) * 32 + l]);
                 }
-                const int idx = first + lane;
-                a.acc[idx] += (double)sx * a.out_scale;
-                a.acc[(size_t)a.npart + idx] += (double)sy * a.out_scale;
-                a.acc[2 * (size_t)a.npart + idx] += (double)sz * a.out_scale;
+                const int idx = first + sk;
+                double *o = a.acc;
+                const size_t n = (size_t)a.npart;
+                if (W > 1) {  // other warps add their shares of the row to the same sinks
+                    atomicAdd(o + idx, (double)sx * a.out_scale);
+                    atomicAdd(o + n + idx, (double)sy * a.out_scale);
+                    atomicAdd(o + 2 * n + idx, (double)sz * a.out_scale);
+                } else {
+                    o[idx] += (double)sx * a.out_scale;
+                    o[n + idx] += (double)sy * a.out_scale;
+                    o[2 * n + idx] += (double)sz * a.out_scale;
+                }
             }
             __syncwarp();  // accumulators and stage are rewritten by the next slice
             evaluated += (unsigned long long)staged * (unsigned long long)ns;

@@ -24,6 +24,7 @@ VARIANT_SOURCE_LANES_X2 = 3
 VARIANT_SOURCE_LANES_X2_S16 = 4
 VARIANT_SINK_LANES_X2 = 5
 VARIANT_SINK_REGS = 6
+VARIANT_SINK_REGS8 = 7
 
 FORM_NAMES = {
     FORM_PLAIN_FP64: "plain_fp64",
@@ -46,6 +47,7 @@ class Params(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_int),
         ("kernel_variant", ctypes.c_int),
         ("poly_tol", ctypes.c_double),
+        ("warps_per_leaf", ctypes.c_int),
     ]
 
 

@@ -1,7 +1,11 @@
 """Launch-shape autotuner of the pair kernel, keyed on the leaf-size histogram.
 
 The shape of a pass is (mapping and sink tile, sources staged per warp,
-warps per block): the packed source-lane kernel holds a slice of a sink leaf
+warps per block, warps per sink leaf): the sink-register kernel keeps four
+sinks per lane in registers over 32-sink slices (SINK_REGS) or eight over
+64-sink slices (SINK_REGS8, so leaves of up to 64 particles stage their
+sources once), and spreads one sink leaf's row over 1, 2 or 4 warps
+(warps_per_leaf, partial forces added with atomics); the packed source-lane kernel holds a slice of a sink leaf
 in registers against one staged source per lane (32 sinks, SOURCE_LANES_X2,
 or 16 sinks with half the partial registers and more resident warps,
 SOURCE_LANES_X2_S16); the packed sink-lane kernel keeps one sink pair per
@@ -33,7 +37,10 @@ CANDIDATES = [
     (v, st, w) for v in (abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SOURCE_LANES_X2_S16)
     for st in (128, 256, 512) for w in (2, 4)
 ] + [(abi.VARIANT_SINK_LANES_X2, st, w) for st in (128, 256, 512) for w in (2, 4)
-] + [(abi.VARIANT_SINK_REGS, st, w) for st in (256, 384) for w in (2, 4)]
+] + [(abi.VARIANT_SINK_REGS, st, w, lw) for st in (256, 384) for w in (2, 4) for lw in (1, 2, 4)
+] + [(abi.VARIANT_SINK_REGS8, st, w, lw) for st in (256, 384) for w in (2, 4) for lw in (1, 2)]
+# every candidate as (variant, stage, warps per block, warps per leaf)
+CANDIDATES = [c if len(c) == 4 else c + (1,) for c in CANDIDATES]
 
 
 def histogram_key(leaf_npart, task_t, form, soft_mode):
@@ -89,6 +96,7 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, re
     def apply(rec):
         p = params_for(cfg, form, mass)
         p.kernel_variant, p.stage_sources, p.warps_per_block = rec["variant"], rec["stage"], rec["warps"]
+        p.warps_per_leaf = rec.get("leaf_warps", 1)
         return p
 
     if key in cache:
@@ -100,12 +108,14 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, re
     args = (lists.npart, d[0].data_ptr(), lists.nleaf, d[1].data_ptr(), d[2].data_ptr(), len(st),
             d[3].data_ptr(), d[4].data_ptr())
     results = []
-    cands = candidates if form != abi.FORM_PLAIN_FP64 else [(0, st_, w) for st_ in (64, 128, 256)
+    cands = candidates if form != abi.FORM_PLAIN_FP64 else [(0, st_, w, 1) for st_ in (64, 128, 256)
                                                               for w in (2, 4, 8)]
     with Session(device) as s:
-        for variant, stage, warps in cands:
+        for cand in cands:
+            variant, stage, warps, lw = cand if len(cand) == 4 else tuple(cand) + (1,)
             p = params_for(cfg, form, mass)
             p.kernel_variant, p.stage_sources, p.warps_per_block = variant, stage, warps
+            p.warps_per_leaf = lw
             try:
                 s.set_params(p)
                 ms = []
@@ -115,13 +125,13 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, re
                     ms.append(s.last_kernel_ms())
             except Exception as e:  # a shape that does not fit is skipped
                 if log:
-                    log(f"[tune] {variant}/{stage}/{warps}: {e}")
+                    log(f"[tune] {variant}/{stage}/{warps}/{lw}: {e}")
                 continue
             t = min(ms[1:])
-            results.append({"variant": variant, "stage": stage, "warps": warps, "kernel_ms": t,
-                            "pairs_per_s": pairs / (t * 1e-3)})
+            results.append({"variant": variant, "stage": stage, "warps": warps, "leaf_warps": lw,
+                            "kernel_ms": t, "pairs_per_s": pairs / (t * 1e-3)})
             if log:
-                log(f"[tune] variant {variant} stage {stage} warps {warps}: {t:.3f} ms "
+                log(f"[tune] variant {variant} stage {stage} warps {warps} warps/leaf {lw}: {t:.3f} ms "
                     f"{pairs / (t * 1e-3):.3e} pairs/s")
     best = max(results, key=lambda r: r["pairs_per_s"])
     rec = dict(best, sample_pairs=pairs, candidates=len(results))

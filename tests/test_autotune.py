@@ -65,10 +65,13 @@ def test_cache_round_trip(tmp_path):
 
 def test_candidates_cover_the_configured_axes():
     """Every packed mapping is a candidate, with several stage sizes and
-    block shapes each."""
-    variants = {v for v, _, _ in autotune.CANDIDATES}
+    block shapes each; the sink-register kernel with 32- and 64-sink tiles
+    and 1, 2 and 4 warps per sink leaf."""
+    assert all(len(c) == 4 for c in autotune.CANDIDATES)
+    variants = {c[0] for c in autotune.CANDIDATES}
     assert {abi.VARIANT_SOURCE_LANES_X2, abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2,
-            abi.VARIANT_SINK_REGS} <= variants
+            abi.VARIANT_SINK_REGS, abi.VARIANT_SINK_REGS8} <= variants
     for v in variants:
-        shapes = {(st, w) for vv, st, w in autotune.CANDIDATES if vv == v}
+        shapes = {(st, w) for vv, st, w, _ in autotune.CANDIDATES if vv == v}
         assert len({st for st, _ in shapes}) >= 2 and len({w for _, w in shapes}) >= 2
+    assert {lw for v, _, _, lw in autotune.CANDIDATES if v == abi.VARIANT_SINK_REGS} == {1, 2, 4}

@@ -74,7 +74,8 @@ def test_plain_matches_oracle_c1_plummer(gpu, c1):
 
 
 VARIANTS = [abi.VARIANT_SINK_LANES, abi.VARIANT_SOURCE_LANES, abi.VARIANT_SOURCE_LANES_X2,
-            abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2, abi.VARIANT_SINK_REGS]
+            abi.VARIANT_SOURCE_LANES_X2_S16, abi.VARIANT_SINK_LANES_X2, abi.VARIANT_SINK_REGS,
+            abi.VARIANT_SINK_REGS8]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -150,6 +151,38 @@ def test_launch_shapes(gpu, dropin32, warps, stage, bps, variant):
                      blocks_per_sm=bps, kernel_variant=variant)
     rms, mx = rel_err(got, ref, tl.tag == 1)
     assert mx <= 1e-5, (rms, mx)
+
+
+@pytest.mark.parametrize("variant", [abi.VARIANT_SINK_REGS, abi.VARIANT_SINK_REGS8])
+@pytest.mark.parametrize("leaf_warps", [2, 4])
+@pytest.mark.parametrize("maxleaf", [32, 64])
+def test_warps_per_leaf(gpu, variant, leaf_warps, maxleaf):
+    """A sink leaf's row spread over 2 or 4 warps (each a contiguous share of
+    its entries, partial forces added with atomics), with 32- and 64-sink
+    tiles, at leaf caps 32 and 64: the same forces as one warp per leaf (to
+    the atomics' reassociation) and within the FP32 form's bars of the FP64
+    form; pair counts unchanged."""
+    cfg = W.ref_dropin_config(32, 64, maxleaf)
+    pos = W.lattice_gaussian(32, 0.2, W.rng(5))
+    tl = W.prepare(pos, cfg)
+    m = 1.0 / pos.shape[1]
+    one, p1 = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, kernel_variant=abi.VARIANT_SINK_REGS)
+    got, p2 = gpu_acc(cfg, tl, m, abi.FORM_SPLIT, kernel_variant=variant, warps_per_leaf=leaf_warps)
+    assert p1 == p2
+    rms, mx = rel_err(got, one, tl.tag == 1)
+    assert mx <= 1e-5, (rms, mx)
+    plain, _ = gpu_acc(cfg, tl, m, abi.FORM_PLAIN_FP64)
+    rms, mx = rel_err(got, plain, tl.tag == 1)
+    assert rms <= SPLIT_RMS and mx <= SPLIT_MAX, (rms, mx)
+
+
+def test_warps_per_leaf_rejects_other_values(gpu):
+    cfg = W.ref_dropin_config(32, 64, 32)
+    with Session(0) as s:
+        prm = params_for(cfg, abi.FORM_SPLIT, 1.0)
+        prm.warps_per_leaf = 3
+        with pytest.raises(P2PError):
+            s.set_params(prm)
 
 
 def test_big_leaves_maxleaf256(gpu):
