@@ -997,7 +997,8 @@ def main():
     ap.add_argument("--side", type=int, default=512, help="c3: particles per side")
     ap.add_argument("--leaf-caps", default="16,32,64", help="c3: leaf caps to sweep")
     ap.add_argument("--chunk-rows", type=float, default=1.0e9, help="c3: list entries per chunk")
-    ap.add_argument("--tune-pairs", type=float, default=2e9, help="c3: autotuner sample size")
+    ap.add_argument("--tune-pairs", type=float, default=1e10,
+                    help="autotuner sample size (pair interactions; enough rows that every warp gets several)")
     ap.add_argument("--tune-cache", default=None, help="c3: autotuner cache (JSON)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -19,7 +19,9 @@ mean list entries per sink leaf, leaf cap) plus the form and softening.
 
 tune() times every candidate on a sample of the pass (the rows of every
 k-th sink leaf, about `sample_pairs` pair interactions) with CUDA events and
-keeps the fastest.
+keeps the fastest. The default sample, 1e10 pairs, gives every resident warp
+many sink leaves: with a few per warp the tail of uneven rows dominates and
+spreading a row over several warps wins on the sample but not on the pass.
 """
 import json
 import os
@@ -83,7 +85,7 @@ def save_cache(path, cache):
     os.replace(tmp, path)
 
 
-def tune(cfg, lists, form, mass, device=0, sample_pairs=2e9, cache_path=None, repeats=2,
+def tune(cfg, lists, form, mass, device=0, sample_pairs=1e10, cache_path=None, repeats=2,
          candidates=CANDIDATES, log=None):
     """Best launch shape for this pass; returns (params, record). With
     cache_path, a cached record under the same key is reused and new results
