@@ -339,8 +339,9 @@ int p2p_session_last_kernel_ms(p2p_session *s, float *ms);
  * on that stream (it reads the pass's status word there); other streams and
  * the rest of the device are not synchronised. The numeric fields of params
  * are checked as p2p_session_set_params checks them; warps_per_block,
- * blocks_per_sm and kernel_variant are ignored (the split form always runs
- * the packed source-lane kernel, 4 warps per block, as many blocks as fit).
+ * blocks_per_sm, kernel_variant and warps_per_leaf are ignored (the split
+ * form always runs the packed source-lane kernel, 4 warps per block, as many
+ * blocks as fit, one warp per sink leaf).
  *
  * Limit: the scratch needed, about 16*npart (split form only) + 48*nleaf +
  * 4*ntask bytes plus 256-byte alignment of each piece, must fit in
