@@ -242,10 +242,24 @@ __global__ void fmm_upward_kernel(FmmArgs f) {
     }
 }
 
+// Whether an opened pair's child can lead to a task: two leaves (a P2P pair)
+// and a pair beyond the cutoff (acceptance -1) end the recursion with none,
+// so they are not written to the next level. Codes outside the tree are
+// kept, for the next level to report.
+__device__ __forceinline__ bool walk_child_live(const WalkArgs &w, int A, int B) {
+    if (A < 0 || B < 0) return false;
+    if (!walk_valid(w, A) || !walk_valid(w, B)) return true;
+    if (A == B) return (A & 1) != 0;
+    if (!(A & 1) && !(B & 1)) return false;
+    return walk_acceptance(walk_width(w, A), walk_width(w, B), walk_center(w, A), walk_center(w, B), w.cutoff,
+                           w.open_angle) != -1;
+}
+
 // One level of the M2L walk: each pending pair is accepted (a task), opened
-// into its child pairs, or dropped, as walk_task_m2l decides. Output slots
-// come from warp-aggregated atomics; a level whose outputs exceed the
-// buffers only counts them (the host grows the buffers and repeats it).
+// into its child pairs, or dropped, as walk_task_m2l decides; children that
+// cannot lead to a task are not kept (walk_child_live). Output slots come
+// from warp-aggregated atomics; a level whose outputs exceed the buffers
+// only counts them (the host grows the buffers and repeats it).
 __global__ void fmm_walk_kernel(WalkArgs w, const int2 *__restrict__ in, int nin, int2 *__restrict__ out,
                                 long long out_cap, unsigned long long *nout, int2 *__restrict__ tasks,
                                 long long task_cap, unsigned long long *ntask, int *status) {
@@ -297,6 +311,12 @@ __global__ void fmm_walk_kernel(WalkArgs w, const int2 *__restrict__ in, int nin
                     }
                 }
             }
+        }
+        {  // keep the live children only
+            int m = 0;
+            for (int c = 0; c < nk; ++c)
+                if (walk_child_live(w, kids[c].x, kids[c].y)) kids[m++] = kids[c];
+            nk = m;
         }
         // warp-aggregated output slots
         int kin = nk, tin = nt;
