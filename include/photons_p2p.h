@@ -79,8 +79,8 @@ typedef struct {
 } p2p_params;
 
 /* Lane mappings of the FP32 pair kernel. */
-#define P2P_VARIANT_AUTO 0            /* the session's fastest mapping (P2P_VARIANT_SINK_REGS);
-                                         the ensemble server's P2P_VARIANT_SOURCE_LANES_X2 */
+#define P2P_VARIANT_AUTO 0            /* the fastest mapping, P2P_VARIANT_SINK_REGS (session and
+                                         ensemble server) */
 #define P2P_VARIANT_SINK_LANES 1      /* one lane per sink particle, sources broadcast */
 #define P2P_VARIANT_SOURCE_LANES 2    /* one lane per staged source, sinks broadcast */
 #define P2P_VARIANT_SOURCE_LANES_X2 3 /* source lanes, two sinks per packed f32x2 instruction,

