@@ -36,6 +36,20 @@ void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time)
  * src/fmm.c:1250, :1334). The argument is the reference's P2PPack array. */
 void *p2ppack_compute_gpu(void *packs, int npack);
 
+/* Active-level passes (hierarchical time steps): only the particles of
+ * active_level receive forces (acc[d][j] += result where active_level == -1
+ * or (active_level != 0 and part[j].act == active_level); built with
+ * ACT_OPT, the chunked form also requires (unsigned char) part[j].act ==
+ * (unsigned char) active_level). The call that ends the pass (last_time = 1;
+ * every call of the multi-pack form) also waits for it and adds the result,
+ * as get_last_kntime + hostmalloc_out + devMemcpyDH_updateAcc + hostfree_out
+ * would. Rows whose sink leaf holds no such particle are not computed.
+ * Replace task_compute_p2p_act_gpu, src/gpu_active.impl.h:1-153, and
+ * p2ppack_compute_act_gpu, :155-321 (compiled into src/gpu_entry.cu:388; the
+ * chunked form's one call site, src/fmm.c:1020, is commented out there). */
+void *task_compute_p2p_act_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time, int active_level);
+void *p2ppack_compute_act_gpu(void *packs, int npack, int active_level);
+
 /* Host task buffers the walk writes into (the globals task_t / task_s of
  * src/global.c:128-129). Replace src/gpu_func.impl.h:184-197. */
 void hostmalloc_task(int len_task);

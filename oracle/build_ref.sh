@@ -6,10 +6,11 @@
 #                    + oracle/ref_entry_record.c (records the lists)
 #   libref_pair.so   reference pair arithmetic (src/gpu_kernel.impl.h) host-compiled
 #                    in three variants (FP64, FP64+GPUCUTOFF, FP32 SPI+GPUCUTOFF)
-#   libref_dropin.so reference walk + harness + the B200 drop-in gpu_entry
+#   libref_dropin_{dp,sp,act}.so reference walk + harness + the B200 drop-in gpu_entry
 #                    (photons-on-mt3000_b200/csrc/gpu_entry_b200.cpp) + the multi-pack
 #                    harness oracle/ref_pack_harness.c, linked to libphotons_p2p.so;
-#                    built only when that library exists.
+#                    built only when that library exists (act: the FP64 form built
+#                    with ACT_OPT, the reference's active-level sink filter).
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]
 #   REFERENCE_ROOT defaults to $PHOTONS_REFERENCE, else /root/reference.
 set -euo pipefail
@@ -47,8 +48,10 @@ PKG="$REPO/photons-on-mt3000_b200"
 if [ -f "$PKG/photons_p2p/libphotons_p2p.so" ]; then
   g++ $CFLAGS -std=c++17 -I"$REPO/include" -DGPU_DP -DGPUCUTOFF -c "$PKG/csrc/gpu_entry_b200.cpp" -o "$OBJ/gpu_entry_b200_dp.o"
   g++ $CFLAGS -std=c++17 -I"$REPO/include" -DGPUCUTOFF -c "$PKG/csrc/gpu_entry_b200.cpp" -o "$OBJ/gpu_entry_b200_sp.o"
+  g++ $CFLAGS -std=c++17 -I"$REPO/include" -DGPU_DP -DGPUCUTOFF -DACT_OPT -c "$PKG/csrc/gpu_entry_b200.cpp" \
+    -o "$OBJ/gpu_entry_b200_act.o"
   gcc $CFLAGS -c "$HERE/ref_pack_harness.c" -o "$OBJ/ref_pack_harness.o"
-  for v in dp sp; do
+  for v in dp sp act; do
     g++ -shared -fopenmp -Wl,-Bsymbolic -o "$OUT/libref_dropin_$v.so" $WALK_OBJS "$OBJ/ref_pack_harness.o" "$OBJ/gpu_entry_b200_$v.o" \
       -L"$PKG/photons_p2p" -lphotons_p2p -Wl,-rpath,'$ORIGIN/../../photons-on-mt3000_b200/photons_p2p'
   done

@@ -277,3 +277,36 @@ def ref_pack_run(libname, pos, leaf_ipart, leaf_npart, leaf_base, split_radius, 
     if st != 0:
         raise RuntimeError("pack harness failed")
     return acc, ksec.value
+
+
+def ref_act_run(libname, pos, leaf_ipart, leaf_npart, leaf_base, split_radius, soften, mass, packs, act,
+                active_level, mode, chunk=0, acc0=None):
+    """The drop-in's active-level entries driven through the reference's
+    globals (oracle/ref_pack_harness.c, ref_act_run): mode "pack" calls
+    p2ppack_compute_act_gpu with the packs, mode "task" calls
+    task_compute_p2p_act_gpu over the packs' concatenated entries in chunks
+    of `chunk`. act: the particles' levels (part[i].act). Returns acc0 (3,
+    npart; zeros if None) plus what the call added."""
+    L = ctypes.CDLL(os.path.join(REF_DIR, libname), mode=ctypes.RTLD_LOCAL)
+    f = L.ref_act_run
+    f.restype = ctypes.c_int
+    pos = np.ascontiguousarray(pos, np.float64)
+    n = pos.shape[1]
+    ip = np.ascontiguousarray(leaf_ipart, np.int32)
+    npt = np.ascontiguousarray(leaf_npart, np.int32)
+    col = lambda k: np.ascontiguousarray([p[k] for p in packs], np.int32)  # noqa: E731
+    ntask = np.ascontiguousarray([len(p["task_t"]) for p in packs], np.int32)
+    tt = np.ascontiguousarray(np.concatenate([p["task_t"] for p in packs]), np.int32)
+    ts = np.ascontiguousarray(np.concatenate([p["task_s"] for p in packs]), np.int32)
+    cols = [col(k) for k in ("ileaf", "nleaf", "ipart", "npart")]
+    acc = np.zeros((3, n)) if acc0 is None else np.array(acc0, np.float64, order="C", copy=True)
+    act = np.ascontiguousarray(act, np.int32)
+    assert act.shape == (n,) and acc.shape == (3, n)
+    f.argtypes = ([ctypes.c_int, _vp, ctypes.c_int, _vp, _vp, ctypes.c_int] + [ctypes.c_double] * 3 +
+                  [ctypes.c_int] + [_vp] * 9 + [ctypes.c_int] * 3)
+    st = f(n, _p(pos), ip.shape[0], _p(ip), _p(npt), leaf_base, split_radius, soften, mass, len(packs),
+           _p(ntask), *[_p(c) for c in cols], _p(tt), _p(ts), _p(acc), _p(act), {"pack": 1, "task": 2}[mode],
+           active_level, chunk)
+    if st != 0:
+        raise RuntimeError("active-level harness failed")
+    return acc

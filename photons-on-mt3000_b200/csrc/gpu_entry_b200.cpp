@@ -171,9 +171,112 @@ void begin_pass() {
     g_pass_open = true;
 }
 
+// Active-level passes (hierarchical time steps). The particles such a pass
+// changes: the reference's download adds a result where level == -1 or
+// (level != 0 and act == level) (updateAcc_fromHostBuff,
+// src/gpu_func.impl.h:644-653); built with ACT_OPT, the kernel of
+// task_compute_p2p_act_gpu also leaves a sink at zero unless its act, as a
+// byte, equals the level as a byte (P2P_kernel, src/gpu_kernel.impl.h:392-396),
+// so a result it adds there is zero.
+bool act_updates(int act, int level, bool kernel_filter) {
+    if (kernel_filter && (unsigned char)act != (unsigned char)level) return false;
+    return level == -1 || (level != 0 && act == level);
+}
+
+#ifdef ACT_OPT
+constexpr bool kActKernelFilter = true;
+#else
+constexpr bool kActKernelFilter = false;
+#endif
+
+// Per leaf of the pass (0-based): 1 if it holds a particle the active-level
+// pass changes. Only the rows of those sink leaves are submitted: every other
+// row's results the reference computes and then does not add (or adds as
+// zeros), so the sums are the same with less work.
+std::vector<unsigned char> g_leaf_live;
+std::vector<int> g_act_tasks;  // the kept entries of a chunk (pageable: staged by the submit)
+
+void mark_live_leaves(int level, bool kernel_filter) {
+    const int nleaf = last_leaf - first_leaf;
+    g_leaf_live.assign((size_t)(nleaf > 0 ? nleaf : 1), 0);
+#pragma omp parallel for schedule(static)
+    for (int l = 0; l < nleaf; ++l) {
+        const int a = leaf[l + first_leaf].ipart, b = a + leaf[l + first_leaf].npart;
+        unsigned char live = 0;
+        for (int j = a; j < b && !live; ++j) live = act_updates(part[j].act, level, kernel_filter) ? 1 : 0;
+        g_leaf_live[(size_t)l] = live;
+    }
+}
+
+// Copies the entries whose sink leaf is live to t / s as 0-based leaf ids
+// (tin / sin hold ids base-based; t / s must not overlap them), keeping their
+// order; returns how many. Blocks are counted, then filled, in parallel.
+int64_t keep_live_rows(int64_t m, const int *tin, const int *sin, int base, int *t, int *s) {
+    constexpr int kBlocks = 256;
+    int64_t cnt[kBlocks + 1];
+    const int nleaf = last_leaf - first_leaf;
+    auto live = [&](int64_t j) {
+        const int l = tin[j] - base;
+        return l >= 0 && l < nleaf && g_leaf_live[(size_t)l];
+    };
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < kBlocks; ++b) {
+        int64_t c = 0;
+        for (int64_t j = m * b / kBlocks; j < m * (b + 1) / kBlocks; ++j) c += live(j) ? 1 : 0;
+        cnt[b + 1] = c;
+    }
+    cnt[0] = 0;
+    for (int b = 0; b < kBlocks; ++b) cnt[b + 1] += cnt[b];
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < kBlocks; ++b) {
+        int64_t o = cnt[b];
+        for (int64_t j = m * b / kBlocks; j < m * (b + 1) / kBlocks; ++j)
+            if (live(j)) {
+                t[o] = tin[j] - base;
+                s[o] = sin[j] - base;
+                ++o;
+            }
+    }
+    return cnt[kBlocks];
+}
+
+// Each pack's list rebased to 0-based leaf ids into the module's page-locked
+// task staging and submitted to the open pass; with live, only the rows of
+// live sink leaves.
+void submit_packs(P2PPack *packs, int npack, bool live) {
+    size_t total = 0;
+    for (int n = 0; n < npack; ++n) total += (size_t)(packs[n].ntask > 0 ? packs[n].ntask : 0);
+    int *buf = (int *)g_pin_tasks.get(sizeof(int) * 2 * (total > 0 ? total : 1));
+    size_t off = 0;
+    for (int n = 0; n < npack; ++n) {
+        if (packs[n].ntask <= 0) continue;
+        packs[n].rankid = 0;
+        const int m = packs[n].ntask;
+        int *t = buf + 2 * off, *s = t + m;
+        int64_t k = m;
+        if (live) {
+            k = keep_live_rows(m, packs[n].task_t, packs[n].task_s, first_leaf, t, s);
+        } else {
+#pragma omp parallel for schedule(static)
+            for (int j = 0; j < m; ++j) {
+                t[j] = packs[n].task_t[j] - first_leaf;
+                s[j] = packs[n].task_s[j] - first_leaf;
+            }
+        }
+        if (k > 0) check("p2p_pass_submit", p2p_pass_submit(g_sess, k, t, s));
+        off += (size_t)m;
+    }
+}
+
+void update_acc(P2PPack *packs, int npack, int active_level, bool kernel_filter);
+
 }  // namespace
 
 extern "C" {
+
+double get_last_kntime(int proc_rank);
+void hostmalloc_out(int npart);
+void hostfree_out(void);
 
 void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time) {
     const bool first_time = (g_call_cnt == 0);
@@ -218,23 +321,71 @@ void *task_compute_p2p_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time)
 void *p2ppack_compute_gpu(P2PPack *packs, int npack) {
     if (npack == 0) return NULL;
     begin_pass();
-    size_t total = 0;
-    for (int n = 0; n < npack; ++n) total += (size_t)(packs[n].ntask > 0 ? packs[n].ntask : 0);
-    int *buf = (int *)g_pin_tasks.get(sizeof(int) * 2 * (total > 0 ? total : 1));
-    size_t off = 0;
-    for (int n = 0; n < npack; ++n) {
-        if (packs[n].ntask <= 0) continue;
-        packs[n].rankid = 0;
-        const int m = packs[n].ntask;
-        int *t = buf + 2 * off, *s = t + m;
-#pragma omp parallel for schedule(static)
-        for (int j = 0; j < m; ++j) {
-            t[j] = packs[n].task_t[j] - first_leaf;
-            s[j] = packs[n].task_s[j] - first_leaf;
-        }
-        check("p2p_pass_submit", p2p_pass_submit(g_sess, m, t, s));
-        off += (size_t)m;
+    submit_packs(packs, npack, false);
+    return NULL;
+}
+
+// Active-level chunked pass: as task_compute_p2p_gpu, but only the particles
+// of the level receive forces, and the last chunk also ends the pass and adds
+// the result (get_last_kntime, hostmalloc_out, devMemcpyDH_updateAcc and
+// hostfree_out inside the call). Replaces task_compute_p2p_act_gpu,
+// src/gpu_active.impl.h:1-153. Like the reference, it rebases the caller's
+// arrays in place; the rows of sink leaves without a particle of the level
+// are not submitted.
+void *task_compute_p2p_act_gpu(int ntask, int *ltask_t, int *ltask_s, int last_time, int active_level) {
+    const bool first_time = (g_call_cnt == 0);
+    g_tot_tasks += ntask;
+    g_call_cnt++;
+    P2PPack *pack = packlist;
+    pack->ntask = ntask;
+    pack->task_t = ltask_t;
+    pack->task_s = ltask_s;
+    pack->ileaf = first_leaf;
+    pack->nleaf = last_leaf - first_leaf;
+    pack->ipart = 0;
+    pack->npart = NPART;
+    pack->rankid = 0;
+    if (first_time) {
+        NPACK++;
+        begin_pass();
+        mark_live_leaves(active_level, kActKernelFilter);
     }
+    if (ntask > 0) {
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < ntask; ++j) {
+            ltask_t[j] -= first_leaf;
+            ltask_s[j] -= first_leaf;
+        }
+        if (g_act_tasks.size() < 2 * (size_t)ntask) g_act_tasks.resize(2 * (size_t)ntask);
+        int *t = g_act_tasks.data(), *s = t + ntask;
+        const int64_t k = keep_live_rows(ntask, ltask_t, ltask_s, 0, t, s);
+        if (k > 0) check("p2p_pass_submit", p2p_pass_submit(g_sess, k, t, s));
+    }
+    if (last_time) {
+        g_tot_tasks = 0;
+        g_call_cnt = 0;
+        get_last_kntime(PROC_RANK);
+        hostmalloc_out(NPART);
+        update_acc(pack, NPACK, active_level, kActKernelFilter);
+        hostfree_out();
+    }
+    return NULL;
+}
+
+// Multi-pack active-level pass: as p2ppack_compute_gpu, then the pass is
+// ended and its result added for the particles of the level (here the
+// reference's kernel computes every sink; only its download filters).
+// Replaces p2ppack_compute_act_gpu, src/gpu_active.impl.h:155-321. The rows
+// of sink leaves without a particle of the level are not submitted.
+void *p2ppack_compute_act_gpu(P2PPack *packs, int npack, int active_level) {
+    if (npack == 0) return NULL;
+    begin_pass();
+    mark_live_leaves(active_level, false);
+    submit_packs(packs, npack, true);
+    get_last_kntime(PROC_RANK);
+    hostmalloc_out(NPART);
+    update_acc(packs, NPACK, active_level, false);
+    hostfree_out();
     return NULL;
 }
 
@@ -282,6 +433,16 @@ void hostfree_out(void) {
 // particle that some pack covers (pack ranges may overlap: the walk's
 // inter-subtree pack spans the others, src/fmm_LB.c:25-49,215-228).
 void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
+    update_acc(packs, npack, active_level, false);
+}
+
+}  // extern "C"
+
+namespace {
+
+// devMemcpyDH_updateAcc; kernel_filter adds the ACT_OPT sink test of the
+// active-level pass (act_updates).
+void update_acc(P2PPack *packs, int npack, int active_level, bool kernel_filter) {
     if (!g_sess) return;
     bool any = false;
     for (int n = 0; n < npack; ++n) any = any || packs[n].ntask != 0;
@@ -321,7 +482,7 @@ void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
         const int a = lo[r] < 0 ? 0 : lo[r], b = hi[r] > n ? n : hi[r];
 #pragma omp parallel for schedule(static)
         for (int j = a; j < b; ++j) {
-            if (active_level == -1 || (active_level && part[j].act == active_level)) {
+            if (act_updates(part[j].act, active_level, kernel_filter)) {
                 acc[0][j] += g_out[j];
                 acc[1][j] += g_out[(size_t)n + j];
                 acc[2][j] += g_out[2 * (size_t)n + j];
@@ -331,6 +492,10 @@ void devMemcpyDH_updateAcc(P2PPack *packs, int npack, int active_level) {
     free(lo);
 }
 
+}  // namespace
+
+extern "C" {
+
 void devfree(void) {
     if (g_sess) p2p_session_destroy(g_sess);
     g_sess = nullptr;
@@ -338,6 +503,8 @@ void devfree(void) {
     g_pin_leaf.release();
     g_pin_tasks.release();
     g_pin_out.release();
+    std::vector<unsigned char>().swap(g_leaf_live);
+    std::vector<int>().swap(g_act_tasks);
     g_pin_pos_n = -1;
     g_out = nullptr;
     g_out_n = 0;

@@ -66,11 +66,11 @@ def test_lists_library_loads():
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "libref_dropin_dp.so")),
                     reason="drop-in harness (reference walk + B200 gpu_entry) not built")
-@pytest.mark.parametrize("variant", ["dp", "sp"])
+@pytest.mark.parametrize("variant", ["dp", "sp", "act"])
 def test_dropin_exports_legacy_entry_points(variant):
     syms = exported(os.path.join(REF, f"libref_dropin_{variant}.so"))
     declared = abi.header_symbols(os.path.join(INCLUDE, "photons_gpu_entry.h"))
-    assert "task_compute_p2p_gpu" in declared
+    assert {"task_compute_p2p_gpu", "task_compute_p2p_act_gpu", "p2ppack_compute_act_gpu"} <= set(declared)
     missing = [s for s in declared if s not in syms]
     assert not missing, missing
     # every symbol resolves at load time (no GPU call is made by loading)

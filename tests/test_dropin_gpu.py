@@ -134,3 +134,63 @@ def test_unmoved_particles_are_not_uploaded_again(gpu):
     d = lib.run(moved, tag, *rest, collect_acc=True)
     assert uploaded() == full
     assert np.array_equal(c["acc"], d["acc"])
+
+
+def act_levels(tl, g):
+    """Time-step levels as a hierarchical stepper assigns them: one level
+    per leaf for most particles (neighbours share a step), 5% of the
+    particles on another level (0-3), 2% on level 255."""
+    n = tl.pos.shape[1]
+    act = np.zeros(n, np.int32)
+    lvl = g.integers(1, 4, tl.nleaf)
+    for l in range(tl.nleaf):
+        act[tl.leaf_ipart[l]:tl.leaf_ipart[l] + tl.leaf_npart[l]] = lvl[l]
+    flip = g.uniform(size=n) < 0.05
+    act[flip] = g.integers(0, 4, int(flip.sum()))
+    act[g.uniform(size=n) < 0.02] = 255
+    return act
+
+
+def act_updates(act, level, kernel_filter):
+    """The particles an active-level pass changes: the reference's download
+    adds where level == -1 or (level != 0 and act == level)
+    (src/gpu_func.impl.h:644-653); with ACT_OPT its chunked pass's kernel
+    leaves a sink at zero unless act and level agree as bytes
+    (src/gpu_kernel.impl.h:392-396)."""
+    upd = (level == -1) | ((level != 0) & (act == level))
+    if kernel_filter:
+        upd &= (act & 0xFF) == (level & 0xFF)
+    return upd
+
+
+@pytest.mark.parametrize("lib,mode,level,chunk", [
+    ("dp", "pack", 2, 0), ("dp", "pack", 0, 0), ("dp", "task", 1, 3000), ("dp", "task", -1, 7919),
+    ("act", "task", 2, 3000), ("act", "task", -1, 5000), ("act", "task", 255, 3000)])
+def test_active_level_entry_points(gpu, lib, mode, level, chunk):
+    """p2ppack_compute_act_gpu and task_compute_p2p_act_gpu
+    (src/gpu_active.impl.h) through the reference's globals: the particles
+    of the level receive the oracle's forces on the whole list (rows whose
+    sink leaf has none of them are not computed), every other particle's acc
+    is left as it was, bit for bit. The act library is the FP64 form built
+    with ACT_OPT."""
+    if not O.ref_available(f"libref_dropin_{lib}.so"):
+        pytest.skip(f"libref_dropin_{lib}.so not built")
+    cfg = W.ref_dropin_config(32, 64, 32)
+    pos = W.lattice_gaussian(32, 0.2, W.rng(1))
+    tl = W.prepare(pos, cfg)
+    mass = 1.0 / pos.shape[1]
+    g = np.random.default_rng(11)
+    act = act_levels(tl, g)
+    leaf_base = 5
+    packs = lb_packs(tl, 4, leaf_base)
+    ref, _ = O.p2p_lists(O.params(cfg.soft_mode, cfg.eps, cfg.split_radius, cfg.x_cut, mass), tl.pos,
+                         tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+    acc0 = g.normal(size=ref.shape) * np.linalg.norm(ref, axis=0)  # each particle's own scale
+    got = O.ref_act_run(f"libref_dropin_{lib}.so", tl.pos, tl.leaf_ipart, tl.leaf_npart, leaf_base,
+                        cfg.split_radius, cfg.eps, mass, packs, act, level, mode, chunk, acc0)
+    upd = act_updates(act, level, lib == "act")
+    if level not in (0, -1):
+        assert 0 < upd.sum() < upd.size
+    assert np.array_equal(got[:, ~upd], acc0[:, ~upd])
+    rms, mx = rel_err(got - acc0, ref, upd & (tl.tag == 1))
+    assert mx <= 1e-11 and rms <= 1e-12, (rms, mx)
