@@ -56,5 +56,16 @@ if [ -f "$PKG/photons_p2p/libphotons_p2p.so" ]; then
       -L"$PKG/photons_p2p" -lphotons_p2p -Wl,-rpath,'$ORIGIN/../../photons-on-mt3000_b200/photons_p2p'
   done
 fi
+# The drop-in over a host stand-in for the pass protocol (oracle/host_session_stub.c):
+# CPU tests of the drop-in's host logic; no CUDA library involved.
+g++ $CFLAGS -std=c++17 -I"$REPO/include" -DGPUCUTOFF -c "$PKG/csrc/gpu_entry_b200.cpp" -o "$OBJ/gpu_entry_b200_host.o"
+g++ $CFLAGS -std=c++17 -I"$REPO/include" -DGPUCUTOFF -DACT_OPT -c "$PKG/csrc/gpu_entry_b200.cpp" \
+  -o "$OBJ/gpu_entry_b200_hostact.o"
+gcc $CFLAGS -I"$REPO/include" -c "$HERE/host_session_stub.c" -o "$OBJ/host_session_stub.o"
+[ -f "$OBJ/ref_pack_harness.o" ] || gcc $CFLAGS -c "$HERE/ref_pack_harness.c" -o "$OBJ/ref_pack_harness.o"
+for v in host hostact; do
+  g++ -shared -fopenmp -Wl,-Bsymbolic -o "$OUT/libref_dropin_$v.so" $WALK_OBJS "$OBJ/ref_pack_harness.o" \
+    "$OBJ/gpu_entry_b200_$v.o" "$OBJ/host_session_stub.o"
+done
 rm -rf "$OBJ"
 echo "build_ref: built $(ls "$OUT" | tr '\n' ' ')"
