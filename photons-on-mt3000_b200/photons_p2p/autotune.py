@@ -19,9 +19,14 @@ mean list entries per sink leaf, leaf cap) plus the form and softening.
 
 tune() times every candidate on a sample of the pass (the rows of every
 k-th sink leaf, about `sample_pairs` pair interactions) with CUDA events and
-keeps the fastest. The default sample, 1e10 pairs, gives every resident warp
-many sink leaves: with a few per warp the tail of uneven rows dominates and
-spreading a row over several warps wins on the sample but not on the pass.
+keeps the fastest. The sample holds about `sample_pairs` pairs (1e10) and
+at least 64 sink leaves per resident warp: with a few per warp the tail of
+uneven rows dominates and spreading a row over several warps wins on the
+sample but not on the pass.
+A shape that spreads rows over several warps adds their partial forces with
+FP64 atomics, so its results do not repeat bit for bit between runs; it is
+kept only when it beats the fastest one-warp shape by more than
+`repeatable_margin` (choose()).
 """
 import json
 import os
@@ -56,13 +61,17 @@ def histogram_key(leaf_npart, task_t, form, soft_mode):
             f"_{abi.FORM_NAMES[form]}_soft{soft_mode}")
 
 
-def sample_rows(leaf_npart, task_t, task_s, sample_pairs):
+def sample_rows(leaf_npart, task_t, task_s, sample_pairs, min_rows=0):
     """The rows of every k-th sink leaf, k chosen so the sample holds about
-    sample_pairs pair interactions (the whole list if it is smaller)."""
+    sample_pairs pair interactions (the whole list if it is smaller) and at
+    least min_rows sink leaves (rows) where the list has them."""
     n = np.asarray(leaf_npart, np.int64)
     tt, ts = np.asarray(task_t), np.asarray(task_s)
     total = float(np.dot(n[tt], n[ts]))
     k = max(1, int(total // max(sample_pairs, 1.0)))
+    if min_rows > 0 and k > 1:
+        nsink = int(np.count_nonzero(np.bincount(tt, minlength=n.size)))
+        k = max(1, min(k, nsink // min_rows))
     if k == 1:
         return tt, ts, int(total)
     keep = (tt % k) == 0
@@ -85,8 +94,30 @@ def save_cache(path, cache):
     os.replace(tmp, path)
 
 
+def choose(results, repeatable_margin=0.03):
+    """The record to keep among timed candidates: the fastest, unless it
+    spreads rows over several warps (leaf_warps > 1) and is not faster than
+    the fastest one-warp candidate by more than repeatable_margin, in which
+    case that one (its results repeat bit for bit)."""
+    best = max(results, key=lambda r: r["pairs_per_s"])
+    one = [r for r in results if r.get("leaf_warps", 1) == 1]
+    if best.get("leaf_warps", 1) > 1 and one:
+        b1 = max(one, key=lambda r: r["pairs_per_s"])
+        if best["pairs_per_s"] <= b1["pairs_per_s"] * (1.0 + repeatable_margin):
+            return b1
+    return best
+
+
+# Sample size by rows: every resident warp of the persistent pair kernel
+# (4 blocks of 4 warps per SM) should take this many sink leaves' rows from
+# the sample, so the tail of uneven rows weighs about as little as in a whole
+# pass (a few rows per warp favour spreading rows over several warps).
+ROWS_PER_WARP = 64
+RESIDENT_WARPS_PER_SM = 16
+
+
 def tune(cfg, lists, form, mass, device=0, sample_pairs=1e10, cache_path=None, repeats=2,
-         candidates=CANDIDATES, log=None):
+         candidates=CANDIDATES, log=None, repeatable_margin=0.03, min_rows=None):
     """Best launch shape for this pass; returns (params, record). With
     cache_path, a cached record under the same key is reused and new results
     are stored."""
@@ -103,8 +134,11 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=1e10, cache_path=None, r
 
     if key in cache:
         return apply(cache[key]), dict(cache[key], key=key, cached=True)
-    st, ss, pairs = sample_rows(lists.leaf_npart, lists.task_t, lists.task_s, sample_pairs)
     dev = torch.device("cuda", device)
+    if min_rows is None:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        min_rows = ROWS_PER_WARP * RESIDENT_WARPS_PER_SM * sms
+    st, ss, pairs = sample_rows(lists.leaf_npart, lists.task_t, lists.task_s, sample_pairs, min_rows)
     d = [torch.from_numpy(np.ascontiguousarray(a)).to(dev)
          for a in (lists.pos, lists.leaf_ipart, lists.leaf_npart, st, ss)]
     args = (lists.npart, d[0].data_ptr(), lists.nleaf, d[1].data_ptr(), d[2].data_ptr(), len(st),
@@ -135,7 +169,7 @@ def tune(cfg, lists, form, mass, device=0, sample_pairs=1e10, cache_path=None, r
             if log:
                 log(f"[tune] variant {variant} stage {stage} warps {warps} warps/leaf {lw}: {t:.3f} ms "
                     f"{pairs / (t * 1e-3):.3e} pairs/s")
-    best = max(results, key=lambda r: r["pairs_per_s"])
+    best = choose(results, repeatable_margin)
     rec = dict(best, sample_pairs=pairs, candidates=len(results))
     if cache_path:
         cache = load_cache(cache_path)

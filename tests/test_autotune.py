@@ -75,3 +75,32 @@ def test_candidates_cover_the_configured_axes():
         shapes = {(st, w) for vv, st, w, _ in autotune.CANDIDATES if vv == v}
         assert len({st for st, _ in shapes}) >= 2 and len({w for _, w in shapes}) >= 2
     assert {lw for v, _, _, lw in autotune.CANDIDATES if v == abi.VARIANT_SINK_REGS} == {1, 2, 4}
+
+
+def test_choose_prefers_repeatable_shapes_within_the_margin():
+    """A row spread over several warps sums with atomics (results vary
+    between runs): such a shape is kept only when it is more than the margin
+    faster than the fastest one-warp shape."""
+    one = {"variant": abi.VARIANT_SINK_REGS, "leaf_warps": 1, "pairs_per_s": 1.00e12}
+    one_slow = {"variant": abi.VARIANT_SINK_REGS8, "leaf_warps": 1, "pairs_per_s": 0.90e12}
+    four_close = {"variant": abi.VARIANT_SINK_REGS, "leaf_warps": 4, "pairs_per_s": 1.02e12}
+    four_far = {"variant": abi.VARIANT_SINK_REGS, "leaf_warps": 4, "pairs_per_s": 1.10e12}
+    assert autotune.choose([one_slow, four_close, one]) is one
+    assert autotune.choose([one, four_far, one_slow]) is four_far
+    assert autotune.choose([four_close, one], repeatable_margin=0.0) is four_close
+    assert autotune.choose([four_close]) is four_close  # no one-warp candidate timed
+    assert autotune.choose([one_slow, one]) is one
+
+
+def test_sample_rows_keeps_enough_rows():
+    """min_rows lowers the stride so the sample holds at least that many
+    sink leaves (the pair target alone would take every 10th)."""
+    n, t, s = lists()
+    total = int(np.dot(n[t].astype(np.int64), n[s]))
+    nsink = np.unique(t).size
+    st, ss, pairs = autotune.sample_rows(n, t, s, total / 10, min_rows=nsink // 4)
+    assert np.unique(st).size >= nsink // 4 - 1
+    k = int(nsink // (nsink // 4))
+    assert np.array_equal(st, t[(t % k) == 0]) and np.array_equal(ss, s[(t % k) == 0])
+    st2, _, _ = autotune.sample_rows(n, t, s, total / 10, min_rows=1)
+    assert np.unique(st2).size < np.unique(st).size  # the pair target rules when min_rows is small

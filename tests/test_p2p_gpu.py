@@ -378,3 +378,27 @@ def test_throughput_probes(gpu):
     assert 10.0 < f32 < 80.0, f32
     assert 5.0 < f64 < 42.0, f64
     assert f64 < f32
+
+
+def test_autotune_on_the_gpu(gpu, dropin32, tmp_path):
+    """tune() times the candidates on a row sample, keeps a shape whose pass
+    matches the FP64 form within the split form's bars, and a second call
+    with the same histogram is answered from the JSON cache."""
+    from photons_p2p import autotune
+
+    cfg, tl, mass = dropin32
+    cache = str(tmp_path / "tune.json")
+    prm, rec = autotune.tune(cfg, tl, abi.FORM_SPLIT, mass, sample_pairs=tl.pair_count() / 4, cache_path=cache,
+                             min_rows=64)
+    assert not rec["cached"] and rec["candidates"] >= len(autotune.CANDIDATES) // 2
+    assert rec["sample_pairs"] < tl.pair_count()
+    assert (prm.kernel_variant, prm.stage_sources, prm.warps_per_block, prm.warps_per_leaf) == \
+        (rec["variant"], rec["stage"], rec["warps"], rec["leaf_warps"])
+    prm2, rec2 = autotune.tune(cfg, tl, abi.FORM_SPLIT, mass, cache_path=cache)
+    assert rec2["cached"] and rec2["variant"] == rec["variant"] and prm2.warps_per_leaf == prm.warps_per_leaf
+    with Session(0) as s:
+        s.set_params(prm)
+        acc, _ = s.force_pass(tl.pos, tl.leaf_ipart, tl.leaf_npart, tl.task_t, tl.task_s)
+    plain, _ = gpu_acc(cfg, tl, mass, abi.FORM_PLAIN_FP64)
+    rms, mx = rel_err(acc, plain, tl.tag == 1)
+    assert rms <= SPLIT_RMS and mx <= SPLIT_MAX, (rms, mx)
