@@ -89,6 +89,7 @@ struct p2p_session {
     DevBuf pos, mass, leaf_ip, leaf_np, task_t, task_s, meta, pos4, counts, fill, row_off,
         row_src, tile_sums, acc, status, queue, pairs, skipped, evaluated, probe;
     DevBuf keys_a, keys_b, vals_b, hist, hoffs, hsums;  // radix sort of the list
+    std::vector<DevBuf> scratch;  // grow-only temporaries of p2p_dtree_build, by request order
     // pass state
     bool in_pass = false;
     int npart = 0, nleaf = 0;
@@ -427,6 +428,13 @@ int check_params(const p2p_params *p) { return validate_params(p); }
 void count_launches(int n) { g_launches += n; }
 cudaError_t allow_large_smem() { return allow_smem_all(); }
 int session_device(const p2p_session *s) { return s ? s->device : 0; }
+
+void *session_scratch(p2p_session *s, int slot, size_t bytes) {
+    if (!s || slot < 0) return nullptr;
+    if ((size_t)slot >= s->scratch.size()) s->scratch.resize((size_t)slot + 1);
+    if (ensure(s, s->scratch[(size_t)slot], bytes) != P2P_OK) return nullptr;
+    return s->scratch[(size_t)slot].p;
+}
 }  // namespace p2p
 
 // ------------------------------------------------------------------ ABI ---
@@ -515,6 +523,8 @@ P2P_API int p2p_session_destroy(p2p_session *s) {
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
+    for (DevBuf &b : s->scratch)
+        if (b.p) cudaFree(b.p);
     cudaEvent_t evs[] = {s->ev_begin, s->ev_end, s->ev_k0, s->ev_k1, s->piece_ready[0], s->piece_ready[1],
                          s->piece_free[0], s->piece_free[1]};
     for (cudaEvent_t ev : evs)

@@ -17,4 +17,10 @@ void count_launches(int n);
 cudaError_t allow_large_smem();
 // The CUDA device of a session.
 int session_device(const p2p_session *s);
+// Device scratch the session keeps between calls: slot k holds at least
+// bytes (grown when smaller, after the session's stream has drained;
+// nullptr with p2p_last_error set when allocation fails). Freed with the
+// session. Callers number their temporaries in request order, so repeated
+// calls of the same size allocate nothing.
+void *session_scratch(p2p_session *s, int slot, size_t bytes);
 }  // namespace p2p

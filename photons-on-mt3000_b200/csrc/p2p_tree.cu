@@ -42,20 +42,17 @@ void free_tree(p2p_dtree *t) {
         if (p) cudaFree(p);
 }
 
-// Device allocations of one build, released on every exit path.
+// Temporaries of one build, in the session's grow-only scratch (one slot
+// per request, numbered in request order): a rebuild of the same size
+// allocates and frees nothing. The build returns only after its last kernel
+// has finished, so the next build may reuse every slot.
 struct Scratch {
-    std::vector<void *> ptrs;
-    ~Scratch() {
-        for (void *p : ptrs) cudaFree(p);
-    }
+    p2p_session *s;
+    int next = 0;
     template <class T>
     bool get(T **out, size_t count) {
-        void *p = nullptr;
-        if (cudaMalloc(&p, sizeof(T) * (count > 0 ? count : 1)) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        ptrs.push_back(p);
+        void *p = session_scratch(s, next++, sizeof(T) * (count > 0 ? count : 1));
+        if (!p) return false;
         *out = (T *)p;
         return true;
     }
@@ -121,7 +118,7 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
     const int64_t cap64 = std::min<int64_t>((int64_t)n + 1, 8LL * n / maxleaf + 1024);
     const int cap = (int)cap64;
 
-    Scratch S;
+    Scratch S{s};
     TreeParts P;
     TreeRec R;
     std::memset(&R, 0, sizeof(R));
@@ -303,7 +300,7 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
     cudaError_t e = cudaMemcpyAsync(t->perm, P.id, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaEventRecord(e1, st);
-    if (e == cudaSuccess) e = cudaEventSynchronize(e1);  // the scratch is freed on return
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);  // the next build may reuse the scratch
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t->build_ms, e0, e1);
     if (e != cudaSuccess) {
         free_tree(t);
