@@ -225,6 +225,15 @@ typedef struct p2p_dtree p2p_dtree;
 int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, const int *d_tag, int maxleaf,
                     double boxsize, p2p_dtree **out);
 int p2p_dtree_free(p2p_dtree *t);
+/* Rebuilds t in place (PhotoNs rebuilds its tree every step): the same tree
+ * p2p_dtree_build makes from these inputs, in t's device arrays where they
+ * are large enough (a rebuild of the same or a smaller size allocates
+ * nothing; the build's temporaries stay in the session's scratch). Device
+ * pointers of t may change: read them again (p2p_dtree_device_arrays,
+ * p2p_dtree_walk_tree). On an error t holds no tree (counts 0) until the
+ * next successful rebuild, and must still be freed. */
+int p2p_dtree_rebuild(p2p_session *s, p2p_dtree *t, int npart, const double *d_pos, const int *d_tag,
+                      int maxleaf, double boxsize);
 /* Sizes and the build's device time (ms, CUDA events; nullable outputs). */
 int p2p_dtree_counts(const p2p_dtree *t, int *npart, int *nleaf, int *nnode, float *build_ms);
 /* Device arrays owned by the tree (nullable outputs): positions in tree

@@ -31,6 +31,7 @@ struct p2p_dtree {
     int *son = nullptr, *node_first = nullptr;
     double *node_center = nullptr, *node_width = nullptr;  // AoS, 3 per node
     float build_ms = 0.f;
+    int cap_part = 0, cap_leaf = 0, cap_node = 0;  // sizes the arrays were allocated for
 };
 
 namespace {
@@ -40,6 +41,10 @@ void free_tree(p2p_dtree *t) {
                     t->leaf_width, t->son, t->node_first, t->node_center, t->node_width};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    t->pos = t->leaf_center = t->leaf_width = t->node_center = t->node_width = nullptr;
+    t->perm = t->leaf_ipart = t->leaf_npart = t->leaf_active = t->son = t->node_first = nullptr;
+    t->cap_part = t->cap_leaf = t->cap_node = 0;
+    t->npart = t->nleaf = t->nnode = 0;
 }
 
 // Temporaries of one build, in the session's grow-only scratch (one slot
@@ -89,13 +94,60 @@ int grid(int64_t n, int threads, int cap) {
 
 }  // namespace
 
-P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, const int *d_tag, int maxleaf,
-                            double boxsize, p2p_dtree **out) {
-    if (!s || !out) return report_error(P2P_ERR_ARG, "null argument");
-    *out = nullptr;
+namespace {
+
+int check_build_args(p2p_session *s, int npart, const double *d_pos, int maxleaf, double boxsize) {
+    if (!s) return report_error(P2P_ERR_ARG, "null argument");
     if (npart <= 0 || !d_pos) return report_error(P2P_ERR_ARG, "tree build needs particles");
     if (maxleaf <= 0) return report_error(P2P_ERR_ARG, "maxleaf must be positive");
     if (!(boxsize > 0.0)) return report_error(P2P_ERR_ARG, "boxsize must be positive");
+    return P2P_OK;
+}
+
+// The tree's arrays for npart particles, nleaf leaves and nnode nodes: kept
+// where they are large enough, else reallocated (with an eighth to spare,
+// so rebuilds whose sizes drift reallocate rarely).
+bool fit_tree(p2p_dtree *tree, int n, int nleaf, int nnode) {
+    auto more = [](int c) { return c + c / 8 + 16; };
+    bool ok = true;
+    if (n > tree->cap_part) {
+        cudaFree(tree->pos);
+        cudaFree(tree->perm);
+        tree->pos = nullptr;
+        tree->perm = nullptr;
+        const int c = more(n);
+        ok = ok && dev_alloc(&tree->pos, 3 * (size_t)c) && dev_alloc(&tree->perm, c);
+        tree->cap_part = ok ? c : 0;
+    }
+    if (ok && nleaf > tree->cap_leaf) {
+        int **iv[] = {&tree->leaf_ipart, &tree->leaf_npart, &tree->leaf_active};
+        double **dv[] = {&tree->leaf_center, &tree->leaf_width};
+        for (int **p : iv) { cudaFree(*p); *p = nullptr; }
+        for (double **p : dv) { cudaFree(*p); *p = nullptr; }
+        const int c = more(nleaf);
+        for (int **p : iv) ok = ok && dev_alloc(p, c);
+        for (double **p : dv) ok = ok && dev_alloc(p, 3 * (size_t)c);
+        tree->cap_leaf = ok ? c : 0;
+    }
+    if (ok && nnode > tree->cap_node) {
+        cudaFree(tree->son);
+        cudaFree(tree->node_first);
+        cudaFree(tree->node_center);
+        cudaFree(tree->node_width);
+        tree->son = tree->node_first = nullptr;
+        tree->node_center = tree->node_width = nullptr;
+        const int c = more(nnode);
+        ok = ok && dev_alloc(&tree->son, 2 * (size_t)c) && dev_alloc(&tree->node_first, c) &&
+             dev_alloc(&tree->node_center, 3 * (size_t)c) && dev_alloc(&tree->node_width, 3 * (size_t)c);
+        tree->cap_node = ok ? c : 0;
+    }
+    return ok;
+}
+
+// Builds into tree (its arrays reused where large enough). On an error the
+// caller discards the tree's contents.
+int build_into(p2p_session *s, p2p_dtree *tree, int npart, const double *d_pos, const int *d_tag, int maxleaf,
+               double boxsize) {
     TREE_CUDA(cudaSetDevice(session_device(s)));
     cudaStream_t st = (cudaStream_t)p2p_session_stream(s);
     cudaEvent_t e0, e1;
@@ -265,21 +317,12 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
     for (int d = 0; d <= maxdepth; ++d) tree_order_kernel<<<gn, 256, 0, st>>>(R, nnode, d);
     launches += 2 * (maxdepth + 1);
 
-    p2p_dtree *t = new p2p_dtree();
+    p2p_dtree *t = tree;
     t->device = session_device(s);
+    if (!fit_tree(t, n, nleaf, nnode)) return report_error(P2P_ERR_NOMEM, "tree build: device allocation failed");
     t->npart = n;
     t->nleaf = nleaf;
     t->nnode = nnode;
-    ok = dev_alloc(&t->pos, 3 * (size_t)n) && dev_alloc(&t->perm, n) && dev_alloc(&t->leaf_ipart, nleaf) &&
-         dev_alloc(&t->leaf_npart, nleaf) && dev_alloc(&t->leaf_active, nleaf) &&
-         dev_alloc(&t->leaf_center, 3 * (size_t)nleaf) && dev_alloc(&t->leaf_width, 3 * (size_t)nleaf) &&
-         dev_alloc(&t->son, 2 * (size_t)nnode) && dev_alloc(&t->node_first, nnode) &&
-         dev_alloc(&t->node_center, 3 * (size_t)nnode) && dev_alloc(&t->node_width, 3 * (size_t)nnode);
-    if (!ok) {
-        free_tree(t);
-        delete t;
-        return report_error(P2P_ERR_NOMEM, "tree build: device allocation failed");
-    }
     tree_emit_kernel<<<gn, 256, 0, st>>>(R, nnode, nleaf, t->son, t->node_first, t->node_center, t->node_width,
                                          t->leaf_ipart, t->leaf_npart, t->leaf_center, t->leaf_width);
     {   // the numbering is consistent before the leaf tables are read
@@ -287,8 +330,6 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
         cudaError_t ce = cudaMemcpyAsync(&status, R.counters + 2, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess || (status & TB_NUMBERING)) {
-            free_tree(t);
-            delete t;
             if (ce != cudaSuccess) return cuda_fail(ce, "tree build");
             return report_error(P2P_ERR_STATE, "tree build: inconsistent node records");
         }
@@ -302,14 +343,41 @@ P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, cons
     if (e == cudaSuccess) e = cudaEventRecord(e1, st);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);  // the next build may reuse the scratch
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t->build_ms, e0, e1);
-    if (e != cudaSuccess) {
+    if (e != cudaSuccess) return cuda_fail(e, "tree build");
+    count_launches(launches);
+    return P2P_OK;
+}
+
+}  // namespace
+
+P2P_API int p2p_dtree_build(p2p_session *s, int npart, const double *d_pos, const int *d_tag, int maxleaf,
+                            double boxsize, p2p_dtree **out) {
+    if (!out) return report_error(P2P_ERR_ARG, "null argument");
+    *out = nullptr;
+    const int st = check_build_args(s, npart, d_pos, maxleaf, boxsize);
+    if (st != P2P_OK) return st;
+    p2p_dtree *t = new p2p_dtree();
+    const int r = build_into(s, t, npart, d_pos, d_tag, maxleaf, boxsize);
+    if (r != P2P_OK) {
+        cudaSetDevice(t->device);
         free_tree(t);
         delete t;
-        return cuda_fail(e, "tree build");
+        return r;
     }
-    count_launches(launches);
     *out = t;
     return P2P_OK;
+}
+
+P2P_API int p2p_dtree_rebuild(p2p_session *s, p2p_dtree *t, int npart, const double *d_pos, const int *d_tag,
+                              int maxleaf, double boxsize) {
+    if (!t) return report_error(P2P_ERR_ARG, "null tree");
+    const int st = check_build_args(s, npart, d_pos, maxleaf, boxsize);
+    if (st != P2P_OK) return st;
+    if ((t->pos || t->son) && t->device != session_device(s))
+        return report_error(P2P_ERR_ARG, "tree and session are on different devices");
+    const int r = build_into(s, t, npart, d_pos, d_tag, maxleaf, boxsize);
+    if (r != P2P_OK) t->npart = t->nleaf = t->nnode = 0;  // no tree; its arrays stay for the next rebuild
+    return r;
 }
 
 P2P_API int p2p_dtree_free(p2p_dtree *t) {

@@ -153,6 +153,7 @@ SIGNATURES = {
     "p2p_server_get_stats": (_i, [_vp, ctypes.POINTER(ServerStats)]),
     "p2p_dtree_build": (_i, [_vp, _i, _vp, _vp, _i, _d, ctypes.POINTER(_vp)]),
     "p2p_dtree_free": (_i, [_vp]),
+    "p2p_dtree_rebuild": (_i, [_vp, _vp, _i, _vp, _vp, _i, _d]),
     "p2p_dtree_counts": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                               ctypes.POINTER(ctypes.c_float)]),
     "p2p_dtree_device_arrays": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.POINTER(_vp),

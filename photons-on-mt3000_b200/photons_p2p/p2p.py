@@ -348,6 +348,18 @@ class DeviceTree:
                                                   tag_dev.data_ptr() if tag_dev is not None else None,
                                                   maxleaf, boxsize, ctypes.byref(h)))
         self.h = h
+        self._refresh()
+
+    def rebuild(self, pos_dev, tag_dev, maxleaf, boxsize):
+        """Rebuilds this tree from new positions (p2p_dtree_rebuild), in its
+        device arrays where they are large enough."""
+        n = int(pos_dev.shape[-1])
+        _check(self.lib, self.lib.p2p_dtree_rebuild(self.session.h, self.h, n, pos_dev.data_ptr(),
+                                                    tag_dev.data_ptr() if tag_dev is not None else None,
+                                                    maxleaf, boxsize))
+        self._refresh()
+
+    def _refresh(self):
         a, b, c, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
         _check(self.lib, self.lib.p2p_dtree_counts(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c),
                                                    ctypes.byref(ms)))

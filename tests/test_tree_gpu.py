@@ -109,3 +109,41 @@ def test_pass_on_device_tree_equals_host_lists(gpu):
                 assert np.array_equal(back[:, tl.perm], got)
         rms, mx = rel_err(got, ref, tl.tag == 1)
         assert mx <= (1e-13 if form == abi.FORM_PLAIN_FP64 else 1e-5), (form, rms, mx)
+
+
+def test_rebuild_in_place_equals_fresh_builds(gpu):
+    """p2p_dtree_rebuild: one tree object rebuilt over a sequence of inputs
+    (larger, smaller, the first again, moved particles) equals the host tree
+    of each input entry for entry, and a rebuild that fits the tree's arrays
+    keeps them (no allocation)."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    cases = []
+    for side in (24, 32, 16):
+        cfg = W.ref_dropin_config(side, 2 * side, 32)
+        allpos, tag = W.with_ghosts(W.lattice_gaussian(side, 0.2, W.rng(side)), cfg)
+        cases.append((allpos, tag, cfg))
+    moved = cases[1][0] + W.rng(5).normal(scale=1e-4, size=cases[1][0].shape)
+    cases += [cases[0], (moved, cases[1][1], cases[1][2])]
+    with Session(0) as s:
+        tree = None
+        for i, (pos, tag, cfg) in enumerate(cases):
+            p, t = _dev(pos, torch, dev), _dev(np.asarray(tag, np.int32), torch, dev)
+            if tree is None:
+                tree = DeviceTree(s, p, t, 32, cfg.box)
+            else:
+                before = tree.device_arrays()
+                tree.rebuild(p, t, 32, cfg.box)
+                if i in (2, 3):  # smaller than the largest input so far: the arrays are kept
+                    assert tree.device_arrays() == before
+            d = tree.download()
+            with L.Tree(pos, tag, 32, cfg.box) as host:
+                son, first, center, width = host.nodes()
+                assert tree.npart == pos.shape[1] and tree.nleaf == host.nleaf and tree.nnode == son.shape[0]
+                assert np.array_equal(d["perm"], host.perm) and np.array_equal(d["pos"], host.pos)
+                for k in ("leaf_ipart", "leaf_npart", "leaf_active", "leaf_center", "leaf_width"):
+                    assert np.array_equal(d[k], getattr(host, k)), (i, k)
+                assert np.array_equal(d["son"], son) and np.array_equal(d["node_first"], first)
+                assert np.array_equal(d["node_center"], center) and np.array_equal(d["node_width"], width)
+        tree.close()
