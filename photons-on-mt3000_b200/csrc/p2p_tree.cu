@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -108,7 +109,7 @@ int check_build_args(p2p_session *s, int npart, const double *d_pos, int maxleaf
 // where they are large enough, else reallocated (with an eighth to spare,
 // so rebuilds whose sizes drift reallocate rarely).
 bool fit_tree(p2p_dtree *tree, int n, int nleaf, int nnode) {
-    auto more = [](int c) { return c + c / 8 + 16; };
+    auto more = [](int c) { return (int)std::min<int64_t>((int64_t)c + c / 8 + 16, INT32_MAX); };
     bool ok = true;
     if (n > tree->cap_part) {
         cudaFree(tree->pos);
