@@ -164,25 +164,30 @@ __global__ void csr_scatter_kernel(const int *__restrict__ tt, const int *__rest
 // smaller key at the lower index. Padding a row of length L to the next power
 // of two with +inf keys then never moves a padded key below L, so comparators
 // whose upper index is >= L are simply skipped and no padding is stored.
+// Block sizes and strides are powers of two, so comparator indices are
+// formed with shifts and masks of their logarithms (a division by a run-time
+// value would cost a multi-instruction sequence per comparator).
 template <class Sync>
 __device__ __forceinline__ void flip_bitonic_sort(int *v, int len, int tid, int nthreads,
                                                   Sync sync) {
-    int P = 1;
-    while (P < len) P <<= 1;
-    for (int size = 2; size <= P; size <<= 1) {
-        const int half = size >> 1;
-        for (int i = tid; i < P / 2; i += nthreads) {
-            const int blk = i / half, off = i % half;
-            const int lo = blk * size + off, hi = blk * size + size - 1 - off;
+    int lgP = 0;
+    while ((1 << lgP) < len) ++lgP;
+    const int half_n = (1 << lgP) >> 1;  // comparators per round
+    for (int lgs = 1; lgs <= lgP; ++lgs) {  // merge blocks of 2^lgs keys
+        const int lgh = lgs - 1, hmask = (1 << lgh) - 1, size = 1 << lgs;
+        for (int i = tid; i < half_n; i += nthreads) {
+            const int base = (i >> lgh) << lgs, off = i & hmask;
+            const int lo = base + off, hi = base + size - 1 - off;
             if (hi < len) {
                 const int a = v[lo], b = v[hi];
                 if (a > b) { v[lo] = b; v[hi] = a; }
             }
         }
         sync();
-        for (int stride = half >> 1; stride >= 1; stride >>= 1) {
-            for (int i = tid; i < P / 2; i += nthreads) {
-                const int lo = (i / stride) * 2 * stride + (i % stride), hi = lo + stride;
+        for (int lgst = lgh - 1; lgst >= 0; --lgst) {  // then strides 2^lgst down to 1
+            const int smask = (1 << lgst) - 1;
+            for (int i = tid; i < half_n; i += nthreads) {
+                const int lo = ((i >> lgst) << (lgst + 1)) + (i & smask), hi = lo + (1 << lgst);
                 if (hi < len) {
                     const int a = v[lo], b = v[hi];
                     if (a > b) { v[lo] = b; v[hi] = a; }
