@@ -90,6 +90,7 @@ struct p2p_session {
         row_src, tile_sums, acc, status, queue, pairs, skipped, evaluated, probe;
     DevBuf keys_a, keys_b, vals_b, hist, hoffs, hsums;  // radix sort of the list
     std::vector<DevBuf> scratch;  // grow-only temporaries of p2p_dtree_build, by request order
+    DevBuf walk_slab;             // the walk's first pass keeps short rows here (p2p_pass_submit_walk)
     // pass state
     bool in_pass = false;
     int npart = 0, nleaf = 0;
@@ -135,6 +136,12 @@ int ensure(p2p_session *s, DevBuf &b, size_t bytes) {
 }
 
 bool is_fp32_form(int form) { return form != P2P_FORM_PLAIN_FP64; }
+
+// The device walk's slab of short rows: up to kWalkSlabMax ids per leaf (a
+// power of two, halved down to kWalkSlabMin while it exceeds kWalkSlabBytes).
+constexpr int kWalkSlabMax = 2048;
+constexpr int kWalkSlabMin = 64;
+constexpr size_t kWalkSlabBytes = (size_t)8 << 30;
 
 // Host list submits longer than 2 * kPipePieceMin entries are uploaded and
 // computed in about kPipePieces pieces of at least kPipePieceMin entries.
@@ -519,7 +526,7 @@ P2P_API int p2p_session_destroy(p2p_session *s) {
                       &s->meta, &s->pos4, &s->counts, &s->fill, &s->row_off, &s->row_src,
                       &s->tile_sums, &s->acc, &s->status, &s->queue, &s->pairs, &s->skipped, &s->evaluated, &s->probe,
                       &s->keys_a, &s->keys_b, &s->vals_b, &s->hist, &s->hoffs, &s->hsums,
-                      &s->task_t2, &s->task_s2};
+                      &s->task_t2, &s->task_s2, &s->walk_slab};
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (DevBuf *b : bufs)
         if (b->p) cudaFree(b->p);
@@ -780,9 +787,21 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
     const int threads = kWalkWarps * 32;
     const int grid = grid_for(nleaf, kWalkWarps, s->sm_count * 32);
     int *status = (int *)s->status.p;
-    // pass 1: row lengths, then the row offsets
+    // The first pass keeps each row's first slab_cap entries in a slab of
+    // slab_cap ids per leaf (at most kWalkSlabBytes), from which the rows are
+    // gathered; only rows longer than that are walked a second time.
+    int slab_cap = kWalkSlabMax;
+    while (slab_cap > kWalkSlabMin && (size_t)nleaf * slab_cap * sizeof(int) > kWalkSlabBytes) slab_cap >>= 1;
+    if ((size_t)nleaf * slab_cap * sizeof(int) > kWalkSlabBytes) slab_cap = 0;  // two walks
+    int *slab = nullptr;
+    if (slab_cap > 0) {
+        P2P_TRY(ensure(s, s->walk_slab, sizeof(int) * (size_t)nleaf * slab_cap));
+        slab = (int *)s->walk_slab.p;
+    }
+    // pass 1: row lengths (and the slab), then the row offsets
     walk_rows_kernel<false><<<grid, threads, 0, s->stream>>>(w, (int *)s->counts.p, nullptr, nullptr, nullptr,
-                                                               nullptr, 0.0, 0.f, nullptr, nullptr, status);
+                                                               nullptr, 0.0, 0.f, nullptr, nullptr, status, slab,
+                                                               slab_cap);
     const int ntiles = (int)((nleaf + (int64_t)kScanTile - 1) / kScanTile);
     int64_t *row_off = (int64_t *)s->row_off.p;
     scan_tiles_kernel<<<ntiles, kScanThreads, 0, s->stream>>>((const int *)s->counts.p, nleaf, row_off,
@@ -800,13 +819,20 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
     if (st & ST_WALK_STACK) return fail(P2P_ERR_CAPACITY, "walk: a sink's walk exceeded its stack");
     if (ntask) *ntask = total;
     if (total == 0) return P2P_OK;
-    // pass 2: the rows' source ids, pair counts; then the pair kernel
+    // pass 2: the rows' source ids, pair counts (short rows from the slab,
+    // long rows walked again); then the pair kernel
     P2P_TRY(ensure(s, s->row_src, sizeof(int) * (size_t)total));
     const bool skip = skips_outside(s);
+    const double cscale = 0.5 / s->params.split_radius;
+    const float uout = (float)(s->fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin));
+    unsigned long long *d_skipped = skip ? (unsigned long long *)s->skipped.p : nullptr;
+    if (slab)
+        walk_gather_kernel<<<grid_for(nleaf, 8, s->sm_count * 16), 256, 0, s->stream>>>(
+            (const int *)s->counts.p, row_off, nleaf, slab, slab_cap, (int *)s->row_src.p, s->d_np,
+            (const LeafMeta *)s->meta.p, cscale, uout, (unsigned long long *)s->pairs.p, d_skipped, status);
     walk_rows_kernel<true><<<grid, threads, 0, s->stream>>>(
-        w, nullptr, row_off, (int *)s->row_src.p, s->d_np, (const LeafMeta *)s->meta.p,
-        0.5 / s->params.split_radius, (float)(s->fit.umax * (1.0 + kCutBand) * (1.0 + kOutsideMargin)),
-        (unsigned long long *)s->pairs.p, skip ? (unsigned long long *)s->skipped.p : nullptr, status);
+        w, (int *)s->counts.p, row_off, (int *)s->row_src.p, s->d_np, (const LeafMeta *)s->meta.p, cscale, uout,
+        (unsigned long long *)s->pairs.p, d_skipped, status, nullptr, slab_cap);
     // each row ascending by source leaf id: the serial walk's order for that sink
     int *rs = (int *)s->row_src.p;
     csr_sort_rows_warp_kernel<<<grid_for(nleaf, 4, s->sm_count * 8), 128, 0, s->stream>>>(row_off, nleaf, rs);
@@ -815,7 +841,7 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
     csr_sort_rows_global_kernel<<<grid_for(nleaf, 1, s->sm_count), kSortBlockThreads, 0, s->stream>>>(
         row_off, nleaf, rs);
     CUDA_TRY(cudaGetLastError());
-    launch_count(4);
+    launch_count(slab ? 5 : 4);
     return enqueue_pairs(s, true);
 }
 

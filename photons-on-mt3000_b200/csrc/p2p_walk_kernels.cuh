@@ -93,18 +93,21 @@ __device__ __forceinline__ int walk_child_toward(const WalkArgs &w, int A, int L
 constexpr int kWalkWarps = 4;         // warps (sink leaves in flight) per block
 constexpr int kWalkWarpStack = 1024;  // pending pairs per warp (shared memory)
 
-// One warp per sink leaf. FILL = false: row lengths into counts[L]. FILL =
-// true: the row's source ids into row_src[row_off[L] ...] (in the order the
-// warp finds them; the rows are sorted afterwards), the row's pair count (and,
-// with skipped, the pairs of entries wholly beyond the FP32 forms' cutoff)
-// added into *pairs / *skipped.
+// One warp per sink leaf. FILL = false: row lengths into counts[L]; with a
+// slab, also the row's first slab_cap source ids into slab[L * slab_cap ...]
+// (walk_gather_kernel moves them into the rows). FILL = true: the row's
+// source ids into row_src[row_off[L] ...] (in the order the warp finds them;
+// the rows are sorted afterwards), the row's pair count (and, with skipped,
+// the pairs of entries wholly beyond the FP32 forms' cutoff) added into
+// *pairs / *skipped; with slab_cap > 0 only for the rows longer than
+// slab_cap (counts[L] from the first pass), the others having been gathered.
 template <bool FILL>
 __global__ void __launch_bounds__(kWalkWarps * 32)
 walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__restrict__ row_off,
                  int *__restrict__ row_src, const int *__restrict__ leaf_npart,
                  const LeafMeta *__restrict__ meta, double cscale, float uout,
                  unsigned long long *__restrict__ pairs, unsigned long long *__restrict__ skipped,
-                 int *__restrict__ status) {
+                 int *__restrict__ status, int *__restrict__ slab, int slab_cap) {
     __shared__ int2 stacks[kWalkWarps][kWalkWarpStack];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -115,6 +118,7 @@ walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__re
             if (!FILL && lane == 0) counts[L] = 0;
             continue;
         }
+        if (FILL && slab_cap > 0 && counts[L] <= slab_cap) continue;  // gathered from the slab (warp-uniform)
         if (lane == 0) stk[0] = make_int2(1, 1);  // (root, root): node 0
         __syncwarp();
         int sp = 1, n = 0, bad = 0;
@@ -198,6 +202,7 @@ walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__re
             if (emit) {
                 const int slot = n + __popc(em & lt);
                 const int S = B >> 1;
+                if (!FILL && slab && slot < slab_cap) slab[(int64_t)L * slab_cap + slot] = S;
                 if (FILL) {
                     if (slot < cap) {
                         row_src[base + slot] = S;
@@ -234,6 +239,61 @@ walk_rows_kernel(const WalkArgs w, int *__restrict__ counts, const int64_t *__re
             if (skipped && my_skip) atomicAdd(skipped, my_skip);
         }
     }
+}
+
+// Rows of at most slab_cap entries, from the first pass's slab into their
+// CSR rows (in the order the walk found them; the row sort follows), with the
+// pair counts the fill pass would add. One warp per sink leaf; a row whose
+// offsets disagree with its length, or an id outside the leaves, sets
+// ST_WALK_ROW and is skipped.
+__global__ void __launch_bounds__(256)
+walk_gather_kernel(const int *__restrict__ counts, const int64_t *__restrict__ row_off, int nleaf,
+                   const int *__restrict__ slab, int slab_cap, int *__restrict__ row_src,
+                   const int *__restrict__ leaf_npart, const LeafMeta *__restrict__ meta, double cscale,
+                   float uout, unsigned long long *__restrict__ pairs, unsigned long long *__restrict__ skipped,
+                   int *__restrict__ status) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (int)(((int64_t)gridDim.x * blockDim.x) >> 5);
+    unsigned long long my_pairs = 0, my_skip = 0;
+    int bad = 0;
+    for (int L = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); L < nleaf; L += nw) {
+        const int n = counts[L];
+        if (n <= 0 || n > slab_cap) continue;  // warp-uniform
+        const int64_t base = row_off[L];
+        if (row_off[L + 1] - base != n) {
+            bad = ST_WALK_ROW;
+            continue;
+        }
+        const long long np_t = leaf_npart[L];
+        LeafMeta mt{};
+        if (skipped) mt = meta[L];
+        for (int i = lane; i < n; i += 32) {
+            const int S = slab[(int64_t)L * slab_cap + i];
+            if ((unsigned)S >= (unsigned)nleaf) {
+                bad = ST_WALK_ROW;
+                continue;
+            }
+            row_src[base + i] = S;
+            const unsigned long long np = (unsigned long long)(np_t * (long long)leaf_npart[S]);
+            my_pairs += np;
+            if (skipped) {
+                const LeafMeta ms = meta[S];
+                float ox, oy, oz;
+                entry_offset(ms, mt, cscale, ox, oy, oz);
+                if (entry_u_min(ms, mt, ox, oy, oz) > uout) my_skip += np;
+            }
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        my_pairs += __shfl_xor_sync(kFull, my_pairs, off);
+        my_skip += __shfl_xor_sync(kFull, my_skip, off);
+    }
+    if (lane == 0) {
+        if (my_pairs) atomicAdd(pairs, my_pairs);
+        if (skipped && my_skip) atomicAdd(skipped, my_skip);
+    }
+    if (bad) atomicOr(status, bad);
 }
 
 }  // namespace p2p
