@@ -835,13 +835,16 @@ P2P_API int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *t, double 
         (unsigned long long *)s->pairs.p, d_skipped, status, nullptr, slab_cap);
     // each row ascending by source leaf id: the serial walk's order for that sink
     int *rs = (int *)s->row_src.p;
-    csr_sort_rows_warp_kernel<<<grid_for(nleaf, 4, s->sm_count * 8), 128, 0, s->stream>>>(row_off, nleaf, rs);
-    csr_sort_rows_block_kernel<<<grid_for(nleaf, 1, s->sm_count * 2), kSortBlockThreads, 0, s->stream>>>(
+    csr_sort_rows_warp_kernel<1, kSortWarpMax><<<grid_for(nleaf, 4, s->sm_count * 8), 128, 0, s->stream>>>(
+        row_off, nleaf, rs);
+    csr_sort_rows_warp_kernel<kSortWarpMax, kSortWarpMax2><<<grid_for(nleaf, 4, s->sm_count * 8), 128, 0, s->stream>>>(
+        row_off, nleaf, rs);
+    csr_sort_rows_block_kernel<<<grid_for(nleaf, 1, s->sm_count * 4), kSortBlockThreads, 0, s->stream>>>(
         row_off, nleaf, rs);
     csr_sort_rows_global_kernel<<<grid_for(nleaf, 1, s->sm_count), kSortBlockThreads, 0, s->stream>>>(
         row_off, nleaf, rs);
     CUDA_TRY(cudaGetLastError());
-    launch_count(slab ? 5 : 4);
+    launch_count(slab ? 6 : 5);
     return enqueue_pairs(s, true);
 }
 

@@ -282,8 +282,10 @@ P2P_API int p2p_pass_noalloc(const p2p_params *params, int npart, const double *
     scan_add_kernel<<<grid_cap(nleaf, threads, 1 << 30), threads, 0, s>>>(row_off, nleaf, tiles);
     csr_scatter_kernel<<<eblocks, threads, 0, s>>>(d_task_t, d_task_s, ntask, nleaf, row_off, fill,
                                                    row_src);
-    csr_sort_rows_warp_kernel<<<grid_cap(nleaf, 4, sms * 8), 128, 0, s>>>(row_off, nleaf, row_src);
-    csr_sort_rows_block_kernel<<<grid_cap(nleaf, 1, sms * 2), kSortBlockThreads, 0, s>>>(row_off, nleaf, row_src);
+    csr_sort_rows_warp_kernel<1, kSortWarpMax><<<grid_cap(nleaf, 4, sms * 8), 128, 0, s>>>(row_off, nleaf, row_src);
+    csr_sort_rows_warp_kernel<kSortWarpMax, kSortWarpMax2><<<grid_cap(nleaf, 4, sms * 8), 128, 0, s>>>(row_off, nleaf,
+                                                                                                   row_src);
+    csr_sort_rows_block_kernel<<<grid_cap(nleaf, 1, sms * 4), kSortBlockThreads, 0, s>>>(row_off, nleaf, row_src);
     csr_sort_rows_global_kernel<<<grid_cap(nleaf, 1, sms), kSortBlockThreads, 0, s>>>(row_off, nleaf, row_src);
     if (cudaGetLastError() != cudaSuccess) return fail_after_queue(s, P2P_ERR_CUDA);
 

@@ -199,20 +199,24 @@ __device__ __forceinline__ void flip_bitonic_sort(int *v, int len, int tid, int 
 }
 
 constexpr int kSortWarpMax = 1024;   // rows up to this length: one warp, shared memory
+constexpr int kSortWarpMax2 = 2048;  // rows up to this length: one warp, a larger buffer
 constexpr int kSortBlockMax = 8192;  // rows up to this length: one block, shared memory
 constexpr int kSortBlockThreads = 512;
 
-// Rows of length 2..kSortWarpMax, one warp per row (4 warps per block).
+// Rows of length LO+1..HI (and at least 2), one warp per row (4 warps per
+// block): <1, kSortWarpMax> and <kSortWarpMax, kSortWarpMax2>, so the short
+// rows keep a small buffer and many resident warps.
+template <int LO, int HI>
 __global__ void __launch_bounds__(128)
 csr_sort_rows_warp_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
-    __shared__ int buf[4][kSortWarpMax];
+    __shared__ int buf[4][HI];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int *v = buf[w];
     const int nw = gridDim.x * 4;
     for (int r = blockIdx.x * 4 + w; r < nleaf; r += nw) {
         const int64_t b = row_off[r];
         const int len = (int)(row_off[r + 1] - b);
-        if (len < 2 || len > kSortWarpMax) continue;
+        if (len < 2 || len <= LO || len > HI) continue;
         for (int i = lane; i < len; i += 32) v[i] = row_src[b + i];
         __syncwarp();
         flip_bitonic_sort(v, len, lane, 32, []() { __syncwarp(); });
@@ -221,14 +225,14 @@ csr_sort_rows_warp_kernel(const int64_t *__restrict__ row_off, int nleaf, int *_
     }
 }
 
-// Rows of length kSortWarpMax+1..kSortBlockMax, one block per row.
+// Rows of length kSortWarpMax2+1..kSortBlockMax, one block per row.
 __global__ void __launch_bounds__(kSortBlockThreads)
 csr_sort_rows_block_kernel(const int64_t *__restrict__ row_off, int nleaf, int *__restrict__ row_src) {
     __shared__ int v[kSortBlockMax];
     for (int r = blockIdx.x; r < nleaf; r += gridDim.x) {
         const int64_t b = row_off[r];
         const int len = (int)(row_off[r + 1] - b);
-        if (len <= kSortWarpMax || len > kSortBlockMax) continue;
+        if (len <= kSortWarpMax2 || len > kSortBlockMax) continue;
         for (int i = threadIdx.x; i < len; i += blockDim.x) v[i] = row_src[b + i];
         __syncthreads();
         flip_bitonic_sort(v, len, threadIdx.x, blockDim.x, []() { __syncthreads(); });
