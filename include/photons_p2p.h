@@ -204,7 +204,10 @@ typedef struct p2p_walk_tree {
  * straight into CSR rows equal entry for entry to those p2p_pass_submit
  * builds from the serial walk's list, then the pair kernel runs on them.
  * Within an open pass (its leaves are the tree's leaves). Waits for the row
- * count (one device-to-host read); *ntask (nullable) = list entries.
+ * count (one device-to-host read); *ntask (nullable) = list entries. The
+ * leaves are walked once: rows of up to 2048 entries are kept in a slab the
+ * session holds between passes (2048 ids per leaf, halved while it would
+ * exceed 8 GB) and gathered, longer rows walked a second time.
  * P2P_ERR_ARG for a child code outside the tree, P2P_ERR_CAPACITY when a
  * sink's pending pairs exceed the walk's fixed stack. */
 int p2p_pass_submit_walk(p2p_session *s, const p2p_walk_tree *tree, double cutoff, double open_angle,
