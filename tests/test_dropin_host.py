@@ -3,7 +3,8 @@ gpu_entry_b200.cpp is linked with the reference's globals and walk
 (src/global.c, src/fmm.c) over a host stand-in for the pass protocol
 (oracle/host_session_stub.c) that adds a counting result per submitted entry
 (npart of the source leaf, source id + 1, 1) instead of forces. Sums of small
-integers are exact, so every check is exact: the multi-pack protocol
+integers are exact, so every check is exact: the chunked protocol as the
+reference's own fmm_task drives it, the multi-pack protocol
 (rebasing of absolute leaf ids, an inter-subtree pack overlapping the others),
 the result update over the packs' particles, and the active-level entries'
 row selection and update rule, without and with ACT_OPT. The same entry
@@ -120,3 +121,33 @@ def test_active_level_protocol(tl, lib, mode, level, chunk):
     assert L.stub_passes() == 1
     if level not in (0, -1) or lib == "hostact":
         assert 0 < L.stub_submitted_entries() < tl.ntask  # rows were dropped
+
+
+@pytest.mark.skipif(not O.ref_available("libref_walk.so"), reason="oracle/_ref reference walk not built")
+def test_reference_fmm_task_chunks_through_the_dropin():
+    """The reference's own fmm_prepare / fmm_task (src/fmm.c) calls
+    task_compute_p2p_gpu in LEN_TASK chunks and collects the result as
+    gravity.c does: every entry of its list is submitted once, rebased to
+    0-based leaf ids, across several chunks, and every particle receives its
+    rows' result."""
+    cfg = W.ref_dropin_config(16, 32, 32)
+    allpos, tag = W.with_ghosts(W.lattice_gaussian(16, 0.2, W.rng(3)), cfg)
+    args = (allpos, tag, cfg.maxleaf, cfg.box, cfg.split_radius, cfg.cutoff_radius, cfg.eps, 1.0,
+            cfg.open_angle, 3000)
+    walk = O.RefWalk("libref_walk.so").run(*args)
+    assert len(walk["chunk_end"]) > 1
+    L = stub("host")
+    L.stub_reset()
+    out = O.RefWalk("libref_dropin_host.so").run(*args, collect_acc=True)
+    assert np.array_equal(out["perm"], walk["perm"])
+    nt = len(walk["task_t"])
+    assert L.stub_submitted_entries() == nt and L.stub_passes() == 1
+    ip, npt = walk["leaf_ipart"], walk["leaf_npart"]
+    per_leaf = np.zeros((3, ip.size))
+    np.add.at(per_leaf[0], walk["task_t"], npt[walk["task_s"]])
+    np.add.at(per_leaf[1], walk["task_t"], walk["task_s"] + 1)
+    np.add.at(per_leaf[2], walk["task_t"], 1)
+    want = np.zeros_like(out["acc"])
+    for l in range(ip.size):
+        want[:, ip[l]:ip[l] + npt[l]] = per_leaf[:, l:l + 1]
+    assert np.array_equal(out["acc"], want)
